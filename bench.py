@@ -1,0 +1,344 @@
+"""Benchmark of the SpMV hot path on B200.
+
+Workload (one "step"): y = A x, FP32 plus-times SpMV over the whole R-MAT
+scale-22 graph (4,194,304 vertices, edge factor 16, a/b/c/d = .57/.19/.19/.05,
+self loops and duplicates removed, int32 indices, values and x uniform in
+[0,1), seeded), CSR storage -- the format-sweep configuration at full size.
+
+Metric: achieved SpMV bandwidth in GB/s over algorithmic bytes
+  B = 4 (n+1) [row_ptr] + 8 nnz [col + val] + 4 n [x, read once] + 4 n [y write]
+divided by the device time of one step (CUDA events on the launching
+stream, max over ranks).  Also reported: % of measured HBM peak, GTEPS
+(nnz / t) and the reference's own GB/s formula 16 nnz / t (spmv.cpp:94-98).
+
+  python bench.py [--gpus N --steps K --warmup W] [--format CSR|SELL_C|CSR_SEG|LAV]
+  python bench.py --impl reference   # the reference's OpenMP CPU SpMV, same config
+
+Multi-GPU: the hot path does not need an exchange at these sizes, so
+``--gpus N`` (under torchrun) runs N independent replicas, one per GPU, and
+``value`` sums their work ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SpMV GB/s (% HBM peak) & GTEPS; served-query QPS + p50/p99 vs plain GPU"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--scale", type=int, default=22)
+    p.add_argument("--edge-factor", type=int, default=16)
+    p.add_argument("--graph", default="rmat", choices=["rmat", "er"])
+    p.add_argument("--format", default="CSR", choices=["CSR", "SELL_C", "CSR_SEG", "LAV"])
+    p.add_argument("--seed", type=int, default=42)
+    p.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def hbm_peak():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            return float(json.loads(f.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def make_input(args):
+    from gb_kun_b200 import graphgen as gg
+    if args.graph == "rmat":
+        g = gg.rmat(args.scale, args.edge_factor, seed=args.seed)
+    else:
+        g = gg.uniform(args.scale, args.edge_factor, seed=args.seed)
+    val = gg.values_f32(g, seed=args.seed + 1)
+    x = gg.vector_f32(g.n, seed=args.seed + 2)
+    return g, val, x
+
+
+def alg_bytes(g):
+    return 4 * (g.n + 1) + 8 * g.nnz + 4 * g.n + 4 * g.n
+
+
+def workload_config(args, g):
+    return {"workload": f"spmv_fp32_plus_times_{args.format.lower()}_{args.graph}{args.scale}",
+            "graph": f"{'R-MAT' if args.graph == 'rmat' else 'Erdos-Renyi'} scale {args.scale}, edge factor "
+                     f"{args.edge_factor}, seed {args.seed}",
+            "n": g.n, "nnz": g.nnz, "format": args.format, "index": "int32", "semiring": "plus_times",
+            "l2": "inputs larger than L2 (matrix arrays stream from HBM each step; x is L2-resident by design)"}
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[4 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl" if args.impl == "ours" else "gloo",
+                                timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(args, g, val, x):
+    """The reference's own OpenMP CSR SpMV on this host, bounded sample."""
+    try:
+        from oracle.cpu import Reference
+        if not Reference.available():
+            return None
+        R = Reference()
+        fmt = {"CSR": 0, "SELL_C": 6, "CSR_SEG": 3, "LAV": 4}[args.format]
+        _, ms = R.spmv(g, val, x, fmt=fmt, semiring=0, warmup=1, reps=1)
+        reps = max(3, min(200, int(args.cpu_baseline_seconds * 1000 / max(ms, 1e-3))))
+        _, ms = R.spmv(g, val, x, fmt=fmt, semiring=0, warmup=0, reps=reps)
+        return {"value": alg_bytes(g) / (ms * 1e-3) / 1e9, "unit": "GB/s", "cores": R.max_threads(),
+                "kind": "reference",
+                "sample": f"full matrix, median of {reps} GrB_mxv calls (reference CPU code, "
+                          f"{args.format}, OMP_NUM_THREADS={R.max_threads()})",
+                "ms_per_spmv": ms}
+    except Exception as e:  # reported, never fatal for the GPU number
+        return {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": f"failed: {e}"}
+
+
+def read_traffic(workload):
+    f = ROOT / "profiles" / f"{workload}.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    from gb_kun_b200 import capi
+    capi.init(local)
+    g, val, x = make_input(args)
+    A = capi.Matrix.from_graph(g, val)
+    if args.format != "CSR":
+        A.set_format(args.format)
+    stream = torch.cuda.current_stream()
+    dx = torch.from_numpy(x).cuda()
+    dy = torch.zeros(g.n, device="cuda")
+    B = alg_bytes(g)
+
+    for _ in range(args.warmup):
+        A.mxv(dx, dy)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    l0 = capi.launch_count()
+    with ClockSampler(local) as clk:
+        t_all0 = torch.cuda.Event(enable_timing=True)
+        t_all1 = torch.cuda.Event(enable_timing=True)
+        t_all0.record(stream)
+        for i in range(args.steps):
+            starts[i].record(stream)
+            A.mxv(dx, dy)
+            ends[i].record(stream)
+        t_all1.record(stream)
+        torch.cuda.synchronize()
+    launches = capi.launch_count() - l0
+    barrier(world)
+    torch.cuda.synchronize()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = max_over_ranks(t_all0.elapsed_time(t_all1), world)
+    ms_per_step = total_ms / args.steps
+    avg_kernel_ms = max_over_ranks(sum(step_ms) / len(step_ms), world)
+
+    # end to end through the public API: pinned host x -> device, SpMV, y -> pinned host
+    hx = torch.from_numpy(x).pin_memory()
+    hy = torch.empty(g.n, dtype=torch.float32).pin_memory()
+    for _ in range(2):
+        dx.copy_(hx, non_blocking=True)
+        A.mxv(dx, dy)
+        hy.copy_(dy, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        dx.copy_(hx, non_blocking=True)
+        A.mxv(dx, dy)
+        hy.copy_(dy, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+
+    # correctness of the timed output (checker only)
+    ok = None
+    if rank == 0:
+        from oracle.cpu import Oracle
+        ref = Oracle().spmv_f64(g, val, x)
+        got = hy.numpy().astype(np.float64)
+        ok = float(np.abs(got - ref).sum() / np.abs(ref).sum())
+
+    peak, peak_kind = hbm_peak()
+    achieved = B / (avg_kernel_ms * 1e-3) / 1e9
+    value = world * B / (ms_per_step * 1e-3) / 1e9
+    cfg = workload_config(args, g)
+    cfg["parallelism"] = f"replicas{world}" if world > 1 else "single"
+    out = {
+        "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded R-MAT, generated in-process)",
+        "config": cfg,
+        "pct_hbm_peak": round(100 * achieved / peak, 2),
+        "gteps": round(world * g.nnz / (ms_per_step * 1e-3) / 1e9, 3),
+        "ref_formula_gbs": round(world * 16 * g.nnz / (ms_per_step * 1e-3) / 1e9, 2),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                     if peak_kind == "measured" else "fallback 6650 GB/s",
+                     "traffic": read_traffic(cfg["workload"]),
+                     "kernel": "k_spmv_merge (+ k_spmv_fixup), timed together per step",
+                     "algorithmic_bytes_per_launch": B},
+        "e2e": {"value": round(world * B / (e2e_ms * 1e-3) / 1e9, 2), "unit": "GB/s",
+                "h2d_bytes_per_step": 4 * g.n, "d2h_bytes_per_step": 4 * g.n, "ms_per_step": round(e2e_ms, 5)},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "check_rel_l1_vs_fp64": ok,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args, g, val, x)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    A.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.cpu import Reference
+    if not Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU library not built (oracle/_ref)"}))
+        return
+    g, val, x = make_input(args)
+    R = Reference()
+    fmt = {"CSR": 0, "SELL_C": 6, "CSR_SEG": 3, "LAV": 4}[args.format]
+    steps = max(1, min(args.steps, 20))
+    warm = max(1, min(args.warmup, 3))
+    _, ms = R.spmv(g, val, x, fmt=fmt, semiring=0, warmup=warm, reps=steps)
+    B = alg_bytes(g)
+    value = B / (ms * 1e-3) / 1e9
+    cfg = workload_config(args, g)
+    cfg["parallelism"] = f"openmp{R.max_threads()}"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
+        "steps": steps, "warmup": warm, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded R-MAT, generated in-process)",
+        "config": cfg,
+        "cpu_baseline": {"value": round(value, 2), "unit": "GB/s", "cores": R.max_threads(), "kind": "reference",
+                         "sample": f"full matrix, median of {steps} GrB_mxv calls"},
+        "e2e": {"value": round(value, 2), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

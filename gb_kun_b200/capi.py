@@ -1,0 +1,181 @@
+"""ctypes binding of the gbk C ABI (libgbk.so) for Python callers.
+
+Device vectors are passed as raw device pointers; :mod:`torch` tensors are the
+convenient owner of that memory (``tensor.data_ptr()``) but never cross the
+ABI.  Every non-zero status raises :class:`GbkError` with the library's last
+error text.  There is no CPU fallback: if the CUDA library is missing or no
+sm_100 device is present, calls fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libgbk.so"
+
+# gbk_types.h
+F32, I32, BOOL, I64, F64 = 0, 1, 2, 3, 4
+FMT = {"CSR": 0, "CSR_SEG": 3, "LAV": 4, "SELL_C": 6}
+SEMIRING = {"plus_times": 0, "lor_land": 1, "first_wins": 2, "first_min": 3, "plus_second": 4,
+            "structural_bool": 5, "min_plus": 6, "custom_less_plus": 7, "min_second": 8, "min_noteq": 9,
+            "plus_one": 10}
+BINOP = {"second": 0, "first": 1, "plus": 2, "minus": 3, "times": 4, "div": 5, "min": 6, "max": 7, "lor": 8,
+         "land": 9, "ne": 10, "lt": 11, "one": 12}
+UNOP = {"identity": 0, "abs": 1, "one": 2}
+MASK = {"scmp": 0, "comp": 2, "structure": 4, "str_comp": 5, "default": 6}
+MONOID = {"plus": 0, "min": 1, "max": 2, "lor": 3, "land": 4, "times": 5}
+
+
+class GbkError(RuntimeError):
+    def __init__(self, status: int, where: str, text: str):
+        super().__init__(f"{where}: status {status}: {text}")
+        self.status = status
+
+
+class FormatParams(C.Structure):
+    _fields_ = [("sell_c", C.c_int32), ("sell_sigma", C.c_int32), ("seg_cols", C.c_int32),
+                ("lav_dense_frac", C.c_float)]
+
+
+class MatrixInfo(C.Structure):
+    _fields_ = [("nrows", C.c_int64), ("ncols", C.c_int64), ("nnz", C.c_int64), ("vtype", C.c_int32),
+                ("format", C.c_int32), ("padded_nnz", C.c_int64), ("device_bytes", C.c_int64),
+                ("ntiles", C.c_int64), ("has_csc", C.c_int32)]
+
+
+_LIB = None
+
+
+def _declare(lib):
+    vp, i64, i32, ci = C.c_void_p, C.c_int64, C.c_int32, C.c_int
+    sig = {
+        "gbk_init": ([ci], ci),
+        "gbk_get_last_error": ([C.c_char_p, C.c_size_t], ci),
+        "gbk_launch_count": ([], i64),
+        "gbk_matrix_create_csr": ([C.POINTER(vp), i64, i64, i64, vp, vp, vp, ci, ci, vp], ci),
+        "gbk_matrix_destroy": ([vp], ci),
+        "gbk_matrix_get_info": ([vp, C.POINTER(MatrixInfo)], ci),
+        "gbk_matrix_csr_arrays": ([vp, ci, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), vp], ci),
+        "gbk_matrix_set_format": ([vp, ci, C.POINTER(FormatParams), vp], ci),
+        "gbk_mxv": ([vp, ci, ci, ci, ci, vp, vp, vp, ci, ci, vp], ci),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name, None)
+        if fn is None:
+            continue
+        fn.argtypes = args
+        fn.restype = res
+    return lib
+
+
+def lib():
+    """Load libgbk.so (built in-tree by gb_kun_b200.build)."""
+    global _LIB
+    if _LIB is None:
+        if not LIB_PATH.exists():
+            raise GbkError(-1, "load", f"{LIB_PATH} is missing: run `python -m gb_kun_b200.build`")
+        _LIB = _declare(C.CDLL(str(LIB_PATH)))
+    return _LIB
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    lib().gbk_get_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int, where: str):
+    if status != 0:
+        raise GbkError(status, where, last_error())
+
+
+def init(device: int = 0):
+    check(lib().gbk_init(device), "gbk_init")
+
+
+def launch_count() -> int:
+    return int(lib().gbk_launch_count())
+
+
+def ptr(t) -> C.c_void_p | None:
+    """Device (or host) address of a torch tensor / numpy array, None for None."""
+    if t is None:
+        return None
+    if isinstance(t, np.ndarray):
+        return C.c_void_p(t.ctypes.data)
+    return C.c_void_p(t.data_ptr())
+
+
+def dtype_code(t) -> int:
+    import torch
+    m = {torch.float32: F32, torch.int32: I32, torch.bool: BOOL, torch.uint8: BOOL, torch.int64: I64,
+         torch.float64: F64}
+    return m[t.dtype]
+
+
+def stream_ptr(stream=None):
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+class Matrix:
+    """Device matrix handle (CSR + lazily built CSC + optional format)."""
+
+    def __init__(self, row_ptr: np.ndarray, col: np.ndarray, val: np.ndarray, ncols: int | None = None,
+                 stream=None):
+        row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int32)
+        col = np.ascontiguousarray(col, dtype=np.int32)
+        val = np.ascontiguousarray(val)
+        vt = {np.dtype(np.float32): F32, np.dtype(np.int32): I32}[val.dtype]
+        self.n = len(row_ptr) - 1
+        self.ncols = self.n if ncols is None else ncols
+        self.nnz = int(row_ptr[-1])
+        self.vtype = vt
+        self.h = C.c_void_p()
+        check(lib().gbk_matrix_create_csr(C.byref(self.h), self.n, self.ncols, self.nnz, ptr(row_ptr), ptr(col),
+                                          ptr(val), vt, 0, stream_ptr(stream)), "gbk_matrix_create_csr")
+
+    @classmethod
+    def from_graph(cls, g, val=None, stream=None):
+        if val is None:
+            val = np.ones(g.nnz, dtype=np.float32)
+        return cls(g.row_ptr, g.col, val, stream=stream)
+
+    def close(self):
+        if self.h:
+            lib().gbk_matrix_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> MatrixInfo:
+        inf = MatrixInfo()
+        check(lib().gbk_matrix_get_info(self.h, C.byref(inf)), "gbk_matrix_get_info")
+        return inf
+
+    def set_format(self, fmt: str, sell_c=0, sigma=0, seg_cols=0, lav_frac=0.0, stream=None):
+        p = FormatParams(sell_c, sigma, seg_cols, lav_frac)
+        check(lib().gbk_matrix_set_format(self.h, FMT[fmt], C.byref(p), stream_ptr(stream)), "gbk_matrix_set_format")
+
+    def arrays(self, transpose=False, stream=None):
+        p, i, v = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(lib().gbk_matrix_csr_arrays(self.h, int(transpose), C.byref(p), C.byref(i), C.byref(v),
+                                          stream_ptr(stream)), "gbk_matrix_csr_arrays")
+        return p.value, i.value, v.value
+
+    def mxv(self, x, y, semiring="plus_times", accum="second", mask=None, mask_mode="default", transpose=False,
+            stream=None):
+        """y = accum(y, A x) (transpose=False) or accum(y, A^T x) on device tensors."""
+        check(lib().gbk_mxv(self.h, int(transpose), SEMIRING[semiring], BINOP[accum], dtype_code(y), ptr(x), ptr(y),
+                            ptr(mask), dtype_code(mask) if mask is not None else 0, MASK[mask_mode],
+                            stream_ptr(stream)), "gbk_mxv")
+        return y

@@ -1,0 +1,72 @@
+// Internal (non-ABI) declarations shared by the CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "gbk.h"
+
+namespace gbk {
+
+// Merge-path tiling of one CSR orientation: tile t covers merge diagonals
+// [t * kTileItems, (t + 1) * kTileItems) of the merged (row-end, nnz) list.
+constexpr int kSpmvThreads = 256;
+constexpr int kSpmvItems = 8;
+constexpr int kTileItems = kSpmvThreads * kSpmvItems;
+
+struct CsrView {
+    int64_t nrows = 0, ncols = 0, nnz = 0;
+    int32_t* ptr = nullptr;  // nrows + 1
+    int32_t* idx = nullptr;  // nnz
+    void* val = nullptr;     // nnz of the matrix value type
+    // merge-path tiles
+    int64_t ntiles = 0;
+    int2* tile_coord = nullptr;  // ntiles + 1 (row, nnz) start coordinates
+    // per-tile carries for rows that cross tiles (scratch, kept with the view)
+    int32_t* carry_row = nullptr;  // ntiles
+    void* carry_val = nullptr;     // ntiles elements (4 bytes each)
+    void* head_val = nullptr;      // ntiles elements
+};
+
+struct SellC;     // spmv_formats.cu
+struct SegCsr;    // spmv_formats.cu
+struct LavMatrix; // spmv_formats.cu
+
+}  // namespace gbk
+
+struct gbk_matrix_s {
+    gbk_dtype vtype = GBK_F32;
+    gbk::CsrView csr;           // A
+    gbk::CsrView csc;           // A^T (built lazily)
+    bool has_csc = false;
+    gbk_format format = GBK_FMT_CSR;
+    gbk_format_params params{};
+    gbk::SellC* sell[2] = {nullptr, nullptr};
+    gbk::SegCsr* seg[2] = {nullptr, nullptr};
+    gbk::LavMatrix* lav[2] = {nullptr, nullptr};
+    void* xcopy = nullptr;      // n elements, used when x aliases y
+    int64_t xcopy_elems = 0;
+    int device = 0;
+};
+
+namespace gbk {
+
+int ensure_csc(gbk_matrix A, cudaStream_t s);
+int build_tiles(CsrView& v, int elem_bytes, cudaStream_t s);
+void free_view(CsrView& v);
+int free_formats(gbk_matrix A);
+
+// SpMV on one CSR orientation (merge-path); y = accum(y, A x) with optional
+// dense mask.  Defined in spmv_csr.cu.
+int spmv_csr(const CsrView& v, int sr, int accum, int dtype, const void* x, void* y, const void* mask,
+             int mask_dtype, int mask_mode, cudaStream_t s);
+
+// Storage-format SpMV (unmasked), defined in spmv_formats.cu.
+int spmv_format(gbk_matrix A, int transpose, int sr, int accum, int dtype, const void* x, void* y,
+                cudaStream_t s);
+int build_format(gbk_matrix A, gbk_format fmt, const gbk_format_params* p, cudaStream_t s);
+size_t format_bytes(gbk_matrix A);
+int64_t format_padded_nnz(gbk_matrix A);
+
+}  // namespace gbk
