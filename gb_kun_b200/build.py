@@ -33,6 +33,7 @@ CU_SOURCES = [
     "spmv_formats.cu",
     "spmspv.cu",
     "vector_ops.cu",
+    "spgemm.cu",
     "batched.cu",
 ]
 

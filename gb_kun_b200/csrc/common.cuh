@@ -85,6 +85,8 @@ __device__ __forceinline__ int32_t elem_add(int32_t a, int32_t b) {
     return (int32_t)s;
 }
 __device__ __forceinline__ float elem_add(float a, float b) { return a + b; }
+__device__ __forceinline__ int64_t elem_add(int64_t a, int64_t b) { return a + b; }
+__device__ __forceinline__ double elem_add(double a, double b) { return a + b; }
 
 // ----------------------------------------------------------------------------
 // semirings (src/cpp_graphblas/types.hpp:274-284): identity / add / mul,

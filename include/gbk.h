@@ -35,6 +35,17 @@ typedef struct gbk_format_params {
     float lav_dense_frac;    /* LAV: fraction of nnz in the dense column segments; default 0.8 */
 } gbk_format_params;
 
+/* A mask argument: either dense (n entries of `dtype`, non-zero = set) or
+ * sparse (`nvals` ascending vertex ids), the two forms backend::Vector
+ * switches between (src/backend/vector/vector.h:81-129). */
+typedef struct gbk_mask {
+    const void* dense;    /* NULL when the mask is sparse */
+    int32_t dtype;        /* gbk_dtype of `dense` */
+    int32_t mode;         /* gbk_mask_mode */
+    const int32_t* ids;   /* sparse form; used when dense == NULL */
+    int64_t nvals;
+} gbk_mask;
+
 typedef struct gbk_matrix_info {
     int64_t nrows, ncols, nnz;
     int32_t vtype;           /* gbk_dtype */
@@ -86,6 +97,100 @@ int gbk_matrix_set_format(gbk_matrix A, gbk_format fmt, const gbk_format_params*
  * use the optimised format chosen by gbk_matrix_set_format.  x may alias y. */
 int gbk_mxv(gbk_matrix A, int transpose, gbk_semiring sr, gbk_binop accum, gbk_dtype dtype, const void* x,
             void* y, const void* mask, gbk_dtype mask_dtype, gbk_mask_mode mask_mode, void* stream);
+
+/* gbk_mxv with a sparse mask: rows listed in mask_ids get accum(y, result)
+ * and other rows keep y, unless mask_mode is GBK_MASK_STR_COMP, where listed
+ * rows get 0 and the others accum(y, result) (SpMV_sparse,
+ * src/backend/spmv/spmv_csr.h:175-262). */
+int gbk_mxv_sparse_mask(gbk_matrix A, int transpose, gbk_semiring sr, gbk_binop accum, gbk_dtype dtype,
+                        const void* x, void* y, const int32_t* mask_ids, int64_t mask_nvals, gbk_mask_mode mask_mode,
+                        void* stream);
+
+/* Push SpMSpV: y = identity, then for every frontier entry (i, x_i) and
+ * every stored A(r, i) (transpose = 0, mxv: the CSC column i) or A(i, r)
+ * (transpose = 1, vxm: the CSR row i): y_r = add(y_r, mul(A, x_i)).  The
+ * update is chosen as the reference does by probing add(3, 5): 8 -> atomic
+ * add, 1 -> store 1, else an atomic read-modify-write with add
+ * (src/backend/spmspv/spmspv.h:103-158, spmspv_atomics.h:5-170).  With a
+ * mask, apply_mask follows (spmspv.h:17-99): selected rows get
+ * accum(old y, y), other rows 0 (a sparse mask without complement leaves
+ * unlisted rows as computed).  Without a mask the accumulator is not used. */
+int gbk_spmspv(gbk_matrix A, int transpose, gbk_semiring sr, gbk_binop accum, gbk_dtype dtype,
+               const int32_t* x_ids, const void* x_vals, int64_t x_nvals, void* y, const gbk_mask* mask,
+               void* stream);
+
+/* ---- SpGEMM ------------------------------------------------------------- */
+
+/* Masked SpGEMM C<M> = A (+.x) B: C gets the structure of M and, at every
+ * stored (i, j) of M, the semiring sum over k in row i of A and column j
+ * of B (GBK_PLUS_ONE counts common k, GBK_PLUS_TIMES sums products).
+ * Replaces SpMSpM_masked_ikj (src/backend/spmspm/spmspm_masked_hash_based_gustavson.h:9-168)
+ * as used by Burkhardt triangle counting (algorithms/tc/tc.hpp:209-217).
+ * Rows of A must be column-sorted (lablas::Matrix keeps them so); B's
+ * columns are read from its device CSC.  *out is a new matrix of ctype
+ * (GBK_I32 or GBK_F32) values. */
+int gbk_mxm_masked(gbk_matrix* out, gbk_matrix M, gbk_matrix A, gbk_matrix B, gbk_semiring sr, gbk_dtype ctype,
+                   void* stream);
+
+/* ---- vectors ------------------------------------------------------------ */
+
+/* Count of non-zero entries (DenseVector::get_nvals, dense_vector.hpp:44-52).
+ * Writes *out on the host; synchronises the stream. */
+int gbk_vec_nvals(const void* v, gbk_dtype t, int64_t n, int64_t* out, void* stream);
+/* Dense -> sparse: ids ascending and their values (SparseVector::convert,
+ * sparse_vector.hpp:35-92).  ids / vals need room for n entries.  Writes
+ * *nvals on the host; synchronises the stream. */
+int gbk_vec_to_sparse(const void* dense, gbk_dtype t, int64_t n, int32_t* ids, void* vals, int64_t* nvals,
+                      void* stream);
+/* Sparse -> dense: zero fill, then scatter (DenseVector::convert, dense_vector.hpp:87-102). */
+int gbk_vec_to_dense(const int32_t* ids, const void* vals, int64_t nvals, gbk_dtype t, void* dense, int64_t n,
+                     void* stream);
+/* v[i] = value (set_all_constant); value is exact for int32 and float. */
+int gbk_vec_fill(void* v, gbk_dtype t, int64_t n, double value, void* stream);
+/* v[i] = i (fillAscending). */
+int gbk_vec_iota(void* v, gbk_dtype t, int64_t n, void* stream);
+/* dst[i] = (dt) src[i]. */
+int gbk_vec_cast(const void* src, gbk_dtype st, void* dst, gbk_dtype dt, int64_t n, void* stream);
+
+/* w[i] = op(u[i], v[i]) computed in optype, for every i the mask selects
+ * (eWiseAdd / eWiseMult, operations.h:216-267 via generic_dense_vector_op,
+ * generic_operations.h:119-164: dense masks select non-zero entries,
+ * sparse masks their ids; the mask mode is not consulted).  mask may be NULL. */
+int gbk_ewise(gbk_binop op, gbk_dtype optype, void* w, gbk_dtype wt, const void* u, gbk_dtype ut, const void* v,
+              gbk_dtype vt, int64_t n, const gbk_mask* mask, void* stream);
+/* apply (operations.h:272-341): kind 0 w = unop(u) (op is a gbk_unop);
+ * kind 1 w = op(scalar, u); kind 2 w = op(u, scalar) (op is a gbk_binop). */
+int gbk_apply(int kind, int op, gbk_dtype optype, void* w, gbk_dtype wt, const void* u, gbk_dtype ut,
+              double scalar, int64_t n, const gbk_mask* mask, void* stream);
+/* Scalar assign (operations.h:15-45, 80-112 via generic_dense_vector_op_assign,
+ * generic_operations.h:11-65 and indexed_dense_vector_op_assign,
+ * indexed_operations.h:12-47): w[i] = value for each selected i; a dense
+ * mask selects non-zero entries under DEFAULT / STRUCTURE and zero entries
+ * under STR_COMP, and nothing under COMP / SCMP.  With indices (device
+ * array of nindices entries of index_t), w[idx[k]] = value (a mask, if
+ * any, must then be dense and is tested at idx[k]). */
+int gbk_assign_scalar(void* w, gbk_dtype wt, int64_t n, double value, const gbk_mask* mask, const void* indices,
+                      gbk_dtype index_t, int64_t nindices, void* stream);
+/* Vector assign (operations.h:50-77, 115-147) and assignScatter: w[i] =
+ * accum(w[i], u[j]) with j = i, except for a sparse DEFAULT / STRUCTURE
+ * mask, where i = ids[k] and j = k (the reference reads u at the mask-list
+ * position, generic_operations.h:28-34).  With indices: w[idx[k]] =
+ * accum(w[idx[k]], u[k]); a repeated index takes the largest k, the result
+ * of the sequential order. */
+int gbk_assign_vector(gbk_binop accum, gbk_dtype optype, void* w, gbk_dtype wt, const void* u, gbk_dtype ut,
+                      int64_t n, const gbk_mask* mask, const void* indices, gbk_dtype index_t, int64_t nindices,
+                      void* stream);
+/* extract (operations.h:401-430): with indices, w[i] = accum(w[i], u[idx[i]])
+ * for i < nindices (a dense mask, if any, tested at idx[i]); without,
+ * w[i] = accum(w[i], u[i]) where a dense mask is non-zero, or
+ * w[k] = accum(w[k], u[ids[k]]) for a sparse mask (generic_operations.h:68-113). */
+int gbk_extract(gbk_binop accum, gbk_dtype optype, void* w, gbk_dtype wt, const void* u, gbk_dtype ut, int64_t n,
+                const gbk_mask* mask, const void* indices, gbk_dtype index_t, int64_t nindices, void* stream);
+/* *result (host, of type rt) = monoid fold of u's n entries, starting from
+ * the monoid identity (operations.h:346-378).  Float sums accumulate in
+ * double.  Synchronises the stream. */
+int gbk_reduce(gbk_monoid monoid, gbk_dtype rt, const void* u, gbk_dtype ut, int64_t n, void* result,
+               void* stream);
 
 #ifdef __cplusplus
 }

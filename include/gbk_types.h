@@ -86,6 +86,15 @@ typedef enum gbk_binop {
 /* Unary operators used by apply(). */
 typedef enum gbk_unop { GBK_UOP_IDENTITY = 0, GBK_UOP_ABS = 1, GBK_UOP_ONE = 2 } gbk_unop;
 
+/* Monoids of reduce() (REGISTER_MONOID, types.hpp:208-214). */
+typedef enum gbk_monoid {
+    GBK_MONOID_PLUS = 0,
+    GBK_MONOID_MIN = 1,
+    GBK_MONOID_MAX = 2,
+    GBK_MONOID_LOR = 3,
+    GBK_MONOID_LAND = 4
+} gbk_monoid;
+
 /* Mask modes: values equal Desc_value (types.hpp:31-38). */
 typedef enum gbk_mask_mode {
     GBK_MASK_SCMP = 0,
