@@ -109,8 +109,10 @@ def build_lablas(force=False) -> Path:
     deps = srcs + list((PKG / "lablas").glob("*.hpp")) + list((PKG / "algorithms").glob("*.hpp")) + \
         list(INCLUDE.glob("*.h")) + [PKG / "libgbk.so"]
     if force or _stale(out, deps):
+        cuda = Path(_nvcc()).resolve().parent.parent
         _run([HOST_CXX, "-O2", "-std=c++17", "-fPIC", "-shared", "-I", str(INCLUDE), "-I", str(PKG),
-              "-o", str(out), *map(str, srcs), "-L", str(PKG), "-lgbk", "-Wl,-rpath,$ORIGIN"])
+              "-I", str(cuda / "include"), "-o", str(out), *map(str, srcs), "-L", str(PKG), "-lgbk",
+              "-L", str(cuda / "lib64"), "-lcudart", "-Wl,-rpath,$ORIGIN"])
     return out
 
 

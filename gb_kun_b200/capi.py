@@ -46,12 +46,34 @@ class MatrixInfo(C.Structure):
                 ("ntiles", C.c_int64), ("has_csc", C.c_int32)]
 
 
+class Mask(C.Structure):
+    """gbk_mask: dense (dense != NULL) or sparse (ids, nvals) mask argument."""
+    _fields_ = [("dense", C.c_void_p), ("dtype", C.c_int32), ("mode", C.c_int32), ("ids", C.c_void_p),
+                ("nvals", C.c_int64)]
+
+
 _LIB = None
 
 
 def _declare(lib):
     vp, i64, i32, ci = C.c_void_p, C.c_int64, C.c_int32, C.c_int
+    mp = C.POINTER(Mask)
     sig = {
+        "gbk_mxv_sparse_mask": ([vp, ci, ci, ci, ci, vp, vp, vp, i64, ci, vp], ci),
+        "gbk_spmspv": ([vp, ci, ci, ci, ci, vp, vp, i64, vp, mp, vp], ci),
+        "gbk_mxm_masked": ([C.POINTER(vp), vp, vp, vp, ci, ci, vp], ci),
+        "gbk_vec_nvals": ([vp, ci, i64, C.POINTER(i64), vp], ci),
+        "gbk_vec_to_sparse": ([vp, ci, i64, vp, vp, C.POINTER(i64), vp], ci),
+        "gbk_vec_to_dense": ([vp, vp, i64, ci, vp, i64, vp], ci),
+        "gbk_vec_fill": ([vp, ci, i64, C.c_double, vp], ci),
+        "gbk_vec_iota": ([vp, ci, i64, vp], ci),
+        "gbk_vec_cast": ([vp, ci, vp, ci, i64, vp], ci),
+        "gbk_ewise": ([ci, ci, vp, ci, vp, ci, vp, ci, i64, mp, vp], ci),
+        "gbk_apply": ([ci, ci, ci, vp, ci, vp, ci, C.c_double, i64, mp, vp], ci),
+        "gbk_assign_scalar": ([vp, ci, i64, C.c_double, mp, vp, ci, i64, vp], ci),
+        "gbk_assign_vector": ([ci, ci, vp, ci, vp, ci, i64, mp, vp, ci, i64, vp], ci),
+        "gbk_extract": ([ci, ci, vp, ci, vp, ci, i64, mp, vp, ci, i64, vp], ci),
+        "gbk_reduce": ([ci, ci, vp, ci, i64, vp, vp], ci),
         "gbk_init": ([ci], ci),
         "gbk_get_last_error": ([C.c_char_p, C.c_size_t], ci),
         "gbk_launch_count": ([], i64),
@@ -179,3 +201,102 @@ class Matrix:
                             ptr(mask), dtype_code(mask) if mask is not None else 0, MASK[mask_mode],
                             stream_ptr(stream)), "gbk_mxv")
         return y
+
+    def mxv_sparse_mask(self, x, y, mask_ids, semiring="plus_times", accum="second", mask_mode="default",
+                        transpose=False, stream=None):
+        check(lib().gbk_mxv_sparse_mask(self.h, int(transpose), SEMIRING[semiring], BINOP[accum], dtype_code(y),
+                                        ptr(x), ptr(y), ptr(mask_ids), int(mask_ids.numel()), MASK[mask_mode],
+                                        stream_ptr(stream)), "gbk_mxv_sparse_mask")
+        return y
+
+    def spmspv(self, x_ids, x_vals, y, semiring="lor_land", accum="second", mask=None, transpose=False,
+               stream=None):
+        """Push SpMSpV from the sparse vector (x_ids, x_vals) into dense y."""
+        check(lib().gbk_spmspv(self.h, int(transpose), SEMIRING[semiring], BINOP[accum], dtype_code(y), ptr(x_ids),
+                               ptr(x_vals), int(x_ids.numel()), ptr(y), C.byref(mask) if mask is not None else None,
+                               stream_ptr(stream)), "gbk_spmspv")
+        return y
+
+    def mxm_masked(self, A, B, semiring="plus_one", ctype=I32, stream=None):
+        """C<self> = A (+.x) B with this matrix as the mask; returns a new Matrix."""
+        out = Matrix.__new__(Matrix)
+        out.h = C.c_void_p()
+        check(lib().gbk_mxm_masked(C.byref(out.h), self.h, A.h, B.h, SEMIRING[semiring], ctype, stream_ptr(stream)),
+              "gbk_mxm_masked")
+        out.n, out.ncols, out.nnz, out.vtype = self.n, self.ncols, self.nnz, ctype
+        return out
+
+
+def dense_mask(t, mode="default") -> Mask:
+    return Mask(ptr(t).value, dtype_code(t), MASK[mode], None, 0)
+
+
+def sparse_mask(ids, mode="default") -> Mask:
+    return Mask(None, 0, MASK[mode], ptr(ids).value, int(ids.numel()))
+
+
+def _mp(mask):
+    return C.byref(mask) if mask is not None else None
+
+
+def ewise(op, optype, w, u, v, mask=None, stream=None):
+    check(lib().gbk_ewise(BINOP[op], optype, ptr(w), dtype_code(w), ptr(u), dtype_code(u), ptr(v), dtype_code(v),
+                          w.numel(), _mp(mask), stream_ptr(stream)), "gbk_ewise")
+
+
+def apply(kind, op, optype, w, u, scalar=0.0, mask=None, stream=None):
+    code = UNOP[op] if kind == 0 else BINOP[op]
+    check(lib().gbk_apply(kind, code, optype, ptr(w), dtype_code(w), ptr(u), dtype_code(u), scalar, w.numel(),
+                          _mp(mask), stream_ptr(stream)), "gbk_apply")
+
+
+def assign_scalar(w, value, mask=None, indices=None, stream=None):
+    check(lib().gbk_assign_scalar(ptr(w), dtype_code(w), w.numel(), float(value), _mp(mask), ptr(indices),
+                                  dtype_code(indices) if indices is not None else I64,
+                                  indices.numel() if indices is not None else 0, stream_ptr(stream)),
+          "gbk_assign_scalar")
+
+
+def assign_vector(accum, optype, w, u, mask=None, indices=None, nindices=None, stream=None):
+    ni = (indices.numel() if nindices is None else nindices) if indices is not None else 0
+    check(lib().gbk_assign_vector(BINOP[accum], optype, ptr(w), dtype_code(w), ptr(u), dtype_code(u), w.numel(),
+                                  _mp(mask), ptr(indices), dtype_code(indices) if indices is not None else I64, ni,
+                                  stream_ptr(stream)), "gbk_assign_vector")
+
+
+def extract(accum, optype, w, u, mask=None, indices=None, stream=None):
+    check(lib().gbk_extract(BINOP[accum], optype, ptr(w), dtype_code(w), ptr(u), dtype_code(u), w.numel(),
+                            _mp(mask), ptr(indices), dtype_code(indices) if indices is not None else I64,
+                            indices.numel() if indices is not None else 0, stream_ptr(stream)), "gbk_extract")
+
+
+def reduce(monoid, rt, u, n=None, stream=None):
+    out = {F32: C.c_float, F64: C.c_double, I32: C.c_int32, I64: C.c_int64, BOOL: C.c_uint8}[rt]()
+    check(lib().gbk_reduce(MONOID[monoid], rt, ptr(u), dtype_code(u), u.numel() if n is None else n, C.byref(out),
+                           stream_ptr(stream)), "gbk_reduce")
+    return out.value
+
+
+def to_sparse(dense, stream=None):
+    import torch
+    n = dense.numel()
+    ids = torch.empty(max(n, 1), dtype=torch.int32, device=dense.device)
+    vals = torch.empty(max(n, 1), dtype=dense.dtype, device=dense.device)
+    nv = C.c_int64()
+    check(lib().gbk_vec_to_sparse(ptr(dense), dtype_code(dense), n, ptr(ids), ptr(vals), C.byref(nv),
+                                  stream_ptr(stream)), "gbk_vec_to_sparse")
+    return ids[:nv.value], vals[:nv.value]
+
+
+def to_dense(ids, vals, n, stream=None):
+    import torch
+    out = torch.empty(n, dtype=vals.dtype, device=vals.device)
+    check(lib().gbk_vec_to_dense(ptr(ids), ptr(vals), ids.numel(), dtype_code(vals), ptr(out), n, stream_ptr(stream)),
+          "gbk_vec_to_dense")
+    return out
+
+
+def nvals(v, stream=None) -> int:
+    out = C.c_int64()
+    check(lib().gbk_vec_nvals(ptr(v), dtype_code(v), v.numel(), C.byref(out), stream_ptr(stream)), "gbk_vec_nvals")
+    return out.value

@@ -51,6 +51,18 @@ inline LA_Info done(int rc) { return to_info(rc); }
 
 }  // namespace detail
 
+// Runtime form of the reference's compile-time __DISABLE_SPMSPV__ switch
+// (operations.h:162-166): while set, mxv / vxm always take the SpMV path.
+inline bool& spmspv_disabled() {
+    static thread_local bool v = false;
+    return v;
+}
+struct ScopedDisableSpMSpV {
+    bool old;
+    ScopedDisableSpMSpV() : old(spmspv_disabled()) { spmspv_disabled() = true; }
+    ~ScopedDisableSpMSpV() { spmspv_disabled() = old; }
+};
+
 // ---------------------------------------------------------------------------
 // element-wise (operations.h:216-341)
 
@@ -297,7 +309,7 @@ LA_Info mxv_impl(int transpose, Vector<W>* w, const Vector<M>* mask, BinaryOpTAc
     const gbk_semiring sr = SemiringT::gbk_sr;
     const gbk_binop acc = accum_code<BinaryOpTAccum>();
     const Desc_value mode = mask_mode(desc);
-    bool dense_input = u->is_dense();
+    bool dense_input = u->is_dense() || spmspv_disabled();
 #ifdef __DISABLE_SPMSPV__
     dense_input = true;
 #endif

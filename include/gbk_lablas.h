@@ -1,0 +1,53 @@
+/* Algorithm entry points of libgbk_lablas.so: the reference's graph
+ * algorithms, written against the drop-in lablas:: C++ API
+ * (gb_kun_b200/lablas/gb_kun.h) and run on the GPU.  Plain C for callers in
+ * other languages (the Python tests and bench bind these with ctypes).
+ *
+ * A gbk_lablas_graph holds one CSR graph (int32 indices, host arrays copied
+ * to the device once) as lablas::Matrix<float> and lablas::Matrix<int>.
+ * Every call returns 0 or a gbk_status / LA_Info code; the text of the last
+ * failure of the calling thread is in gbk_lablas_get_last_error.  *ms, when
+ * not NULL, receives the call's wall time in milliseconds with the device
+ * synchronised before and after (graph construction excluded). */
+#ifndef GBK_LABLAS_H
+#define GBK_LABLAS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gbk_lablas_graph_s* gbk_lablas_graph;
+
+/* weights: NULL for unit weights, else nnz int32 edge weights (SSSP). */
+int gbk_lablas_graph_create(gbk_lablas_graph* out, int64_t n, const int32_t* row_ptr, const int32_t* col,
+                            const int32_t* weights);
+int gbk_lablas_graph_destroy(gbk_lablas_graph g);
+int gbk_lablas_get_last_error(char* buf, size_t len);
+
+/* bfs_blast (algorithms/bfs/bfs.hpp:93-142): levels, source = 1, unvisited = 0. */
+int gbk_lablas_bfs(gbk_lablas_graph g, int64_t source, int32_t* levels, double* ms);
+/* FastSV cc (algorithms/cc/cc.hpp:12-119): component labels. */
+int gbk_lablas_cc(gbk_lablas_graph g, int32_t* labels, int32_t* iterations, double* ms);
+/* sssp_bellman_ford_blast (algorithms/sssp/sssp_blast.hpp:8-72) in float
+ * (weights as exact floats; unreachable = FLT_MAX). */
+int gbk_lablas_sssp_f32(gbk_lablas_graph g, int64_t source, float* dist, double* ms);
+/* The same rounds in int32 (unreachable = INT32_MAX). */
+int gbk_lablas_sssp_i32(gbk_lablas_graph g, int64_t source, int32_t* dist, double* ms);
+/* LAGraph page_rank_sinks (algorithms/pr/pr.hpp:20-153); stops after
+ * itermax iterations or once rdiff < tol (tol > 0). */
+int gbk_lablas_pagerank(gbk_lablas_graph g, int32_t itermax, double damping, double tol, float* ranks,
+                        int32_t* iterations, double* ms);
+/* Burkhardt triangle count (algorithms/tc/tc.hpp:209-217); the graph must be symmetric. */
+int gbk_lablas_tc(gbk_lablas_graph g, uint64_t* count, double* ms);
+/* y = A x through lablas::mxv (plus-times, f32) in the given storage format
+ * (MatrixStorageFormat value: 0 CSR, 3 CSR_SEG, 4 LAV, 6 SELL_C); vals are
+ * the nnz matrix values. */
+int gbk_lablas_spmv(gbk_lablas_graph g, int32_t format, const float* vals, const float* x, float* y, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -48,6 +48,15 @@ static double add_elem(double a, double b, int dtype) {
     return narrow(a + b, dtype);
 }
 
+/* Integer multiply / subtract wrap modulo 2^32 as int32 arithmetic does in
+ * the reference's C++ on two's-complement hardware. */
+static double wrap_mul(double a, double b) {
+    return (double)(int32_t)((uint32_t)(int32_t)a * (uint32_t)(int32_t)b);
+}
+static double wrap_sub(double a, double b) {
+    return (double)(int32_t)((uint32_t)(int32_t)a - (uint32_t)(int32_t)b);
+}
+
 static double sr_add(int sr, double a, double b, int dtype) {
     switch (sr) {
         case GBK_PLUS_TIMES:
@@ -75,7 +84,7 @@ static double sr_mul(int sr, double a, double x, int dtype) {
         case GBK_PLUS_TIMES:
         case GBK_FIRST_WINS:
         case GBK_FIRST_MIN:
-            return dtype == ORC_F32 ? (double)((float)a * (float)x) : narrow(a * x, dtype);
+            return dtype == ORC_F32 ? (double)((float)a * (float)x) : wrap_mul(a, x);
         case GBK_LOR_LAND:
             return (a != 0 && x != 0) ? 1.0 : 0.0;
         case GBK_PLUS_SECOND:
@@ -98,8 +107,8 @@ static double binop(int op, double a, double b, int dtype) {
         case GBK_OP_SECOND: return b;
         case GBK_OP_FIRST: return a;
         case GBK_OP_PLUS: return add_elem(a, b, dtype);
-        case GBK_OP_MINUS: return dtype == ORC_F32 ? (double)((float)a - (float)b) : narrow(a - b, dtype);
-        case GBK_OP_TIMES: return dtype == ORC_F32 ? (double)((float)a * (float)b) : narrow(a * b, dtype);
+        case GBK_OP_MINUS: return dtype == ORC_F32 ? (double)((float)a - (float)b) : wrap_sub(a, b);
+        case GBK_OP_TIMES: return dtype == ORC_F32 ? (double)((float)a * (float)b) : wrap_mul(a, b);
         case GBK_OP_DIV:
             if (dtype == ORC_F32) return (double)((float)a / (float)b);
             return b == 0 ? 0.0 : (double)((int32_t)a / (int32_t)b);
