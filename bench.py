@@ -42,8 +42,10 @@ FALLBACK_HBM_GBS = 6650.0
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--steps", type=int, default=2000)
     p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--sweep", action="store_true", help="add the storage-format sweep to the JSON line")
+    p.add_argument("--sweep-steps", type=int, default=200)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--scale", type=int, default=22)
     p.add_argument("--edge-factor", type=int, default=16)
@@ -104,9 +106,13 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()  # the timed region starts once sampling runs
+            while not self.samples and time.time() - t0 < 10:
+                time.sleep(0.02)
+            self.skip = len(self.samples)
         except Exception:
             self.proc = None
         return self
@@ -126,14 +132,15 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.samples:
+        samples = self.samples[getattr(self, "skip", 0):] or self.samples[-1:]
+        if not samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        sm = [float(s[0]) for s in samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in samples if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[4 + i].lower() == "active"})
+        reasons = sorted({names[i] for s in samples for i in range(4) if s[4 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(samples)}
 
 
 def dist_setup(args):
@@ -196,6 +203,62 @@ def read_traffic(workload):
             except ValueError:
                 return None
     return None
+
+
+def time_spmv(A, dx, dy, steps, warmup, semiring="plus_times"):
+    """Average device time (ms) of one SpMV over `steps` launches (CUDA events)."""
+    import torch
+    for _ in range(warmup):
+        A.mxv(dx, dy, semiring=semiring)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        A.mxv(dx, dy, semiring=semiring)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def format_sweep(args, peak):
+    """The format-sweep configuration: every storage format on R-MAT and
+    Erdos-Renyi graphs of the same scale, plus-times and or-and semirings.
+    GB/s counts CSR-equivalent algorithmic bytes (padding is not credited)."""
+    import torch
+    from gb_kun_b200 import capi
+    from gb_kun_b200 import graphgen as gg
+    from oracle.cpu import Oracle
+    O = Oracle()
+    out = {}
+    fmts = [("CSR", {}), ("SELL_C_s1", {"fmt": "SELL_C", "sigma": 1}), ("SELL_C_s256", {"fmt": "SELL_C", "sigma": 256}),
+            ("SELL_C_s4096", {"fmt": "SELL_C", "sigma": 4096}), ("CSR_SEG", {"fmt": "CSR_SEG"}), ("LAV", {"fmt": "LAV"})]
+    for gname in ("rmat", "er"):
+        g = gg.rmat(args.scale, args.edge_factor, seed=args.seed) if gname == "rmat" else \
+            gg.uniform(args.scale, args.edge_factor, seed=args.seed)
+        val = gg.values_f32(g, seed=args.seed + 1)
+        x = gg.vector_f32(g.n, seed=args.seed + 2)
+        ref = O.spmv_f64(g, val, x)
+        B = alg_bytes(g)
+        A = capi.Matrix.from_graph(g, val)
+        dx = torch.from_numpy(x).cuda()
+        dy = torch.zeros(g.n, device="cuda")
+        for name, f in fmts:
+            if f:
+                A.set_format(f["fmt"], sigma=f.get("sigma", 0))
+            else:
+                A.set_format("CSR")
+            ms = time_spmv(A, dx, dy, args.sweep_steps, 3)
+            err = float(np.abs(dy.cpu().numpy().astype(np.float64) - ref).sum() / np.abs(ref).sum())
+            ms_or = time_spmv(A, dx, dy, args.sweep_steps, 3, semiring="lor_land")
+            inf = A.info()
+            out[f"{gname}{args.scale}.{name}"] = {
+                "plus_times_gbs": round(B / (ms * 1e-3) / 1e9, 1), "plus_times_ms": round(ms, 4),
+                "pct_hbm_peak": round(100 * B / (ms * 1e-3) / 1e9 / peak, 1),
+                "or_and_gbs": round(B / (ms_or * 1e-3) / 1e9, 1), "rel_l1_vs_fp64": err,
+                "stored_entries": int(inf.padded_nnz), "nnz": g.nnz}
+        A.close()
+    return out
 
 
 def run_ours(args):
@@ -292,11 +355,13 @@ def run_ours(args):
         "clocks": clk.summary(),
         "check_rel_l1_vs_fp64": ok,
     }
+    A.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args, g, val, x)
+    if args.sweep and rank == 0:
+        out["format_sweep"] = format_sweep(args, peak)
     if rank == 0:
         print(json.dumps(out), flush=True)
-    A.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -228,11 +228,15 @@ class Matrix:
 
 
 def dense_mask(t, mode="default") -> Mask:
-    return Mask(ptr(t).value, dtype_code(t), MASK[mode], None, 0)
+    m = Mask(ptr(t).value, dtype_code(t), MASK[mode], None, 0)
+    m._owner = t  # the mask holds a raw pointer: keep its storage alive
+    return m
 
 
 def sparse_mask(ids, mode="default") -> Mask:
-    return Mask(None, 0, MASK[mode], ptr(ids).value, int(ids.numel()))
+    m = Mask(None, 0, MASK[mode], ptr(ids).value, int(ids.numel()))
+    m._owner = ids
+    return m
 
 
 def _mp(mask):

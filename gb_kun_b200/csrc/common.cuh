@@ -210,6 +210,10 @@ __device__ __forceinline__ bool mask_selects(const void* m, int dtype, int mode,
     return mode == GBK_MASK_STR_COMP ? !v : v;
 }
 
+template <typename T> constexpr int dtype_of_t();
+template <> constexpr int dtype_of_t<float>() { return GBK_F32; }
+template <> constexpr int dtype_of_t<int32_t>() { return GBK_I32; }
+
 inline size_t dtype_size(int dt) {
     switch (dt) {
         case GBK_F32: return 4;

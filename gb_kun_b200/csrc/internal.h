@@ -30,8 +30,7 @@ struct CsrView {
 };
 
 struct SellC;     // spmv_formats.cu
-struct SegCsr;    // spmv_formats.cu
-struct LavMatrix; // spmv_formats.cu
+struct SegCsr;    // spmv_formats.cu (CSR_SEG and LAV share one layout)
 
 }  // namespace gbk
 
@@ -44,7 +43,7 @@ struct gbk_matrix_s {
     gbk_format_params params{};
     gbk::SellC* sell[2] = {nullptr, nullptr};
     gbk::SegCsr* seg[2] = {nullptr, nullptr};
-    gbk::LavMatrix* lav[2] = {nullptr, nullptr};
+    gbk::SegCsr* lav[2] = {nullptr, nullptr};
     void* xcopy = nullptr;      // n elements, used when x aliases y
     int64_t xcopy_elems = 0;
     int device = 0;

@@ -211,6 +211,12 @@ int launch(const CsrView& v, int accum, const void* x, void* y, const void* mask
         GBK_LAUNCHED();
         return GBK_SUCCESS;
     } else {
+        static bool carveout_set = false;  // all shared memory for the tile buffers: 8 CTAs per SM
+        if (!carveout_set) {
+            GBK_CUDA(cudaFuncSetAttribute(k_spmv_merge<SR, T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          cudaSharedmemCarveoutMaxShared));
+            carveout_set = true;
+        }
         k_spmv_merge<SR, T><<<(unsigned)v.ntiles, kSpmvThreads, 0, s>>>(
             v.ptr, v.idx, (const T*)v.val, v.tile_coord, (const T*)x, (T*)y, accum, mask, mdt, mmode, v.carry_row,
             (T*)v.carry_val, (T*)v.head_val);

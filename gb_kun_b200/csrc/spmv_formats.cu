@@ -1,29 +1,791 @@
-// Optimised storage formats (SELL-C-sigma, segmented CSR, LAV).
+// Optimised storage formats: SELL-C-sigma, segmented CSR (CSR_SEG) and LAV.
+//
+// All three are built on the device from the CSR (and, for A^T, the CSC),
+// replacing MatrixSellC::build (src/backend/matrix/containers/sell_c/build.hpp:27-295),
+// MatrixSegmentedCSR::build (seg_csr/build.hpp:23-169) and MatrixLAV::build
+// (lav/build.hpp:3-212), which build serially on the host.
+//
+// SELL-C-sigma (C = 32): rows are sorted by degree, descending, inside
+// windows of sigma rows; slices of 32 consecutive sorted rows are stored
+// column-major and padded to the slice's longest row, so one warp reads one
+// slice with fully coalesced 128-byte loads, lane = row.  Slices the
+// reference calls problematic (padding >= 2x and > 1024 nonzeros,
+// build.hpp:147-155) and slices longer than kSellMaxLen go to an overflow
+// CSR handled by the merge-path kernel, so no warp walks a hub row alone.
+// (The reference computes problematic chunks and then discards the result,
+// spmv_sell_c.h:98-139; here they are computed.)
+//
+// CSR_SEG and LAV: columns are cut into segments (LAV after renumbering
+// columns by descending in-degree and splitting off the 20 % least-used
+// columns as one "sparse" segment).  Each (segment, row) pair with entries
+// becomes one virtual row of a segment-major CSR; the merge-path kernel
+// computes every virtual row, and a merge kernel folds each original row's
+// partials in segment order: y = accum(y, add over segments), as the
+// reference's scatter-merge does (spmv_seg.h:229-298, spmv_lav.h:124-156).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <vector>
+
 #include "common.cuh"
 #include "internal.h"
 
 namespace gbk {
 
+constexpr int kSellC = 32;
+constexpr int kSellMaxLen = 256;
+
+struct SellC {
+    int64_t n = 0;           // rows
+    int64_t nslices = 0;
+    int32_t sigma = 1;
+    int32_t* perm = nullptr;      // sorted position -> row
+    int32_t* slice_len = nullptr; // -1 marks an overflow slice
+    int64_t* slice_ptr = nullptr; // start of each slice in col / val
+    int32_t* col = nullptr;       // column-major padded, -1 = padding
+    void* val = nullptr;
+    int64_t padded = 0;           // stored entries (including padding)
+    // overflow rows (long or problematic slices) as a compact CSR
+    int64_t nov = 0;
+    int32_t* ov_rows = nullptr;   // original row ids
+    CsrView ov;                   // rows 0..nov-1 of the overflow CSR
+    void* ov_out = nullptr;       // nov partial results
+};
+
+struct SegCsr {
+    int64_t n = 0;          // rows of the matrix
+    int64_t nvrows = 0;     // virtual (segment, row) rows
+    int32_t nsegments = 0;
+    CsrView v;              // segment-major virtual CSR
+    int32_t* merge_ptr = nullptr;  // n + 1, into merge_idx
+    int32_t* merge_idx = nullptr;  // virtual rows of each row, in segment order
+    void* partial = nullptr;       // nvrows results
+    int32_t* col_new_to_old = nullptr;  // LAV only: x reorder
+    void* xr = nullptr;                 // LAV only: reordered x (ncols)
+    int64_t ncols = 0;
+};
+
+namespace {
+
+inline unsigned blocks_for(int64_t work, int threads = 256) {
+    int64_t b = (work + threads - 1) / threads;
+    return (unsigned)(b > 0 ? b : 1);
+}
+
+// ---------------------------------------------------------------------------
+// SELL-C kernels
+
+template <int SR, typename T>
+__global__ void __launch_bounds__(256) k_sell_spmv(const int32_t* __restrict__ slice_len,
+                                                   const int64_t* __restrict__ slice_ptr,
+                                                   const int32_t* __restrict__ col, const T* __restrict__ val,
+                                                   const int32_t* __restrict__ perm, int64_t n, int64_t nslices,
+                                                   const T* __restrict__ x, T* __restrict__ y, int accum) {
+    using S = Semiring<SR, T>;
+    const int lane = threadIdx.x & 31;
+    const int64_t s = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (s >= nslices) return;
+    const int len = slice_len[s];
+    if (len < 0) return;  // overflow slice: computed from the overflow CSR
+    const int64_t base = slice_ptr[s] + lane;
+    T acc = S::identity();
+    int j = 0;
+    for (; j + 4 <= len; j += 4) {
+        int c[4];
+        T a[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) c[u] = ld_stream(col + base + (int64_t)(j + u) * kSellC);
+#pragma unroll
+        for (int u = 0; u < 4; u++) a[u] = ld_stream(val + base + (int64_t)(j + u) * kSellC);
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (c[u] >= 0) acc = S::add(acc, S::mul(a[u], ld_reuse(x + c[u])));
+    }
+    for (; j < len; j++) {
+        int c = ld_stream(col + base + (int64_t)j * kSellC);
+        if (c >= 0) acc = S::add(acc, S::mul(ld_stream(val + base + (int64_t)j * kSellC), ld_reuse(x + c)));
+    }
+    const int64_t p = s * kSellC + lane;
+    if (p < n) {
+        const int32_t r = perm[p];
+        y[r] = (accum == GBK_OP_SECOND) ? acc : binop<T>(accum, y[r], acc);
+    }
+}
+
+template <typename T>
+__global__ void k_scatter_rows(const int32_t* __restrict__ rows, const T* __restrict__ part, int64_t nr,
+                               T* __restrict__ y, int accum) {
+    int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k >= nr) return;
+    const int32_t r = rows[k];
+    y[r] = (accum == GBK_OP_SECOND) ? part[k] : binop<T>(accum, y[r], part[k]);
+}
+
+// SELL-C build helpers
+__global__ void k_degrees(const int32_t* ptr, int64_t n, int32_t* deg) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) deg[i] = ptr[i + 1] - ptr[i];
+}
+
+__global__ void k_sigma_keys(const int32_t* deg, int64_t n, int32_t sigma, unsigned long long* keys, int32_t* ids) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    unsigned long long win = (unsigned long long)(i / sigma);
+    keys[i] = (win << 32) | (unsigned long long)(uint32_t)(0x7fffffff - deg[i]);
+    ids[i] = (int32_t)i;
+}
+
+__global__ void k_iota32(int32_t* p, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) p[i] = (int32_t)i;
+}
+
+// one warp per slice: longest row and nonzero count; classify overflow
+__global__ void k_slice_stats(const int32_t* deg, const int32_t* perm, int64_t n, int64_t nslices, int32_t* len,
+                              int64_t* stored, int32_t* is_ov) {
+    const int lane = threadIdx.x & 31;
+    const int64_t s = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (s >= nslices) return;
+    const int64_t p = s * kSellC + lane;
+    int d = (p < n) ? deg[perm[p]] : 0;
+    int mx = d;
+    long long sum = d;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        sum += __shfl_xor_sync(0xffffffffu, sum, off);
+    }
+    if (lane == 0) {
+        const bool problematic = ((long long)mx * kSellC >= 2 * sum) && (sum > 1024);
+        const bool ov = problematic || mx > kSellMaxLen;
+        len[s] = ov ? -1 : mx;
+        stored[s] = ov ? 0 : (int64_t)mx * kSellC;
+        is_ov[s] = ov ? 1 : 0;
+    }
+}
+
+template <typename T>
+__global__ void k_sell_fill(const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx, const T* __restrict__ val,
+                            const int32_t* __restrict__ perm, const int32_t* __restrict__ len,
+                            const int64_t* __restrict__ sptr, int64_t n, int32_t* __restrict__ col,
+                            T* __restrict__ sval) {
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int64_t s = p / kSellC;
+    if (len[s] < 0) return;
+    const int lane = (int)(p % kSellC);
+    const int32_t r = perm[p];
+    const int64_t base = sptr[s] + lane;
+    for (int32_t e = ptr[r], j = 0; e < ptr[r + 1]; e++, j++) {
+        col[base + (int64_t)j * kSellC] = idx[e];
+        sval[base + (int64_t)j * kSellC] = val[e];
+    }
+}
+
+// rows of overflow slices, in sorted order
+__global__ void k_ov_flags(const int32_t* is_ov, const int32_t* perm, int64_t n, int32_t* flag) {
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p < n) flag[p] = is_ov[p / kSellC];
+}
+
+__global__ void k_ov_compact(const int32_t* flag, const int32_t* pos, const int32_t* perm, const int32_t* deg,
+                             int64_t n, int32_t* rows, int32_t* rdeg) {
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p < n && flag[p]) {
+        rows[pos[p]] = perm[p];
+        rdeg[pos[p]] = deg[perm[p]];
+    }
+}
+
+// copy listed rows of a CSR into a compact CSR (warp per row)
+template <typename T>
+__global__ void k_gather_rows(const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                              const T* __restrict__ val, const int32_t* __restrict__ rows,
+                              const int32_t* __restrict__ optr, int64_t nr, int32_t* __restrict__ oidx,
+                              T* __restrict__ oval) {
+    const int lane = threadIdx.x & 31;
+    const int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (k >= nr) return;
+    const int32_t r = rows[k];
+    const int32_t b = ptr[r], e = ptr[r + 1], o = optr[k];
+    for (int32_t q = b + lane; q < e; q += 32) {
+        oidx[o + (q - b)] = idx[q];
+        oval[o + (q - b)] = val[q];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// segmented (CSR_SEG / LAV) kernels
+
+template <int SR, typename T>
+__global__ void k_seg_merge(const int32_t* __restrict__ mptr, const int32_t* __restrict__ midx,
+                            const T* __restrict__ part, int64_t n, T* __restrict__ y, int accum) {
+    using S = Semiring<SR, T>;
+    int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    T acc = S::identity();
+    for (int32_t k = mptr[r]; k < mptr[r + 1]; k++) acc = S::add(acc, part[midx[k]]);
+    y[r] = (accum == GBK_OP_SECOND) ? acc : binop<T>(accum, y[r], acc);
+}
+
+template <typename T>
+__global__ void k_reorder_x(const T* __restrict__ x, const int32_t* __restrict__ new_to_old, int64_t n,
+                            T* __restrict__ xr) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) xr[i] = x[new_to_old[i]];
+}
+
+// Segment id of every entry: key = (segment << 32) | row, value = entry position.
+__global__ void k_seg_keys(const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx, int64_t nrows,
+                           int64_t nnz, const int32_t* __restrict__ col_seg, unsigned long long* __restrict__ keys,
+                           int32_t* __restrict__ pos) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    int64_t lo = 0, hi = nrows;
+    while (hi - lo > 1) {
+        int64_t mid = (lo + hi) >> 1;
+        if (ptr[mid] <= e)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    keys[e] = ((unsigned long long)(uint32_t)col_seg[idx[e]] << 32) | (uint32_t)lo;
+    pos[e] = (int32_t)e;
+}
+
+// virtual-row boundaries: a new virtual row starts where the (segment, row) key changes
+__global__ void k_vrow_flags(const unsigned long long* keys, int64_t nnz, int32_t* flag) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e < nnz) flag[e] = (e == 0 || keys[e] != keys[e - 1]) ? 1 : 0;
+}
+
+template <typename T>
+__global__ void k_vrow_build(const unsigned long long* __restrict__ keys, const int32_t* __restrict__ pos,
+                             const int32_t* __restrict__ flag, const int32_t* __restrict__ vid,
+                             const int32_t* __restrict__ idx, const T* __restrict__ val,
+                             const int32_t* __restrict__ col_map, int64_t nnz, int32_t* __restrict__ vptr,
+                             int32_t* __restrict__ vrow, int32_t* __restrict__ oidx, T* __restrict__ oval,
+                             int32_t* __restrict__ rowcount) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    const int32_t src = pos[e];
+    const int32_t c = idx[src];
+    oidx[e] = col_map ? col_map[c] : c;
+    oval[e] = val[src];
+    if (flag[e]) {
+        const int32_t v = vid[e];  // exclusive scan of flags
+        vptr[v] = (int32_t)e;
+        const int32_t r = (int32_t)(keys[e] & 0xffffffffULL);
+        vrow[v] = r;
+        atomicAdd(&rowcount[r], 1);
+    }
+}
+
+// merge lists: virtual rows of each original row in segment order.  Virtual
+// rows are segment-major, so visiting them in order and appending per row
+// keeps segment order; a per-row cursor does the appending.
+__global__ void k_merge_fill(const int32_t* __restrict__ vrow, int64_t nv, const int32_t* __restrict__ mptr,
+                             int32_t* __restrict__ cursor, int32_t* __restrict__ midx) {
+    int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (v >= nv) return;
+    const int32_t r = vrow[v];
+    const int32_t slot = atomicAdd(&cursor[r], 1);
+    midx[mptr[r] + slot] = (int32_t)v;
+}
+
+// restore segment order inside each row's merge list (short lists: insertion sort)
+__global__ void k_merge_sort(const int32_t* __restrict__ mptr, int64_t n, int32_t* __restrict__ midx) {
+    int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const int32_t b = mptr[r], e = mptr[r + 1];
+    for (int32_t i = b + 1; i < e; i++) {
+        int32_t v = midx[i];
+        int32_t j = i - 1;
+        while (j >= b && midx[j] > v) {
+            midx[j + 1] = midx[j];
+            j--;
+        }
+        midx[j + 1] = v;
+    }
+}
+
+int cub_scan_excl(const int32_t* in, int32_t* out, int64_t n, cudaStream_t s) {
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, (int)n, s);
+    void* tmp = nullptr;
+    GBK_CUDA(cudaMallocAsync(&tmp, tb, s));
+    GBK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, in, out, (int)n, s));
+    count_launch(1);
+    cudaFreeAsync(tmp, s);
+    return GBK_SUCCESS;
+}
+
+int free_sell(SellC* f) {
+    if (!f) return 0;
+    cudaFree(f->perm);
+    cudaFree(f->slice_len);
+    cudaFree(f->slice_ptr);
+    cudaFree(f->col);
+    cudaFree(f->val);
+    cudaFree(f->ov_rows);
+    cudaFree(f->ov_out);
+    free_view(f->ov);
+    delete f;
+    return 0;
+}
+
+int free_seg(SegCsr* f) {
+    if (!f) return 0;
+    free_view(f->v);
+    cudaFree(f->merge_ptr);
+    cudaFree(f->merge_idx);
+    cudaFree(f->partial);
+    cudaFree(f->col_new_to_old);
+    cudaFree(f->xr);
+    delete f;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// SELL-C build
+
+template <typename T>
+int build_sell(const CsrView& a, int32_t sigma, SellC** out, cudaStream_t s) {
+    SellC* f = new SellC();
+    f->n = a.nrows;
+    f->sigma = sigma;
+    const int64_t n = a.nrows;
+    f->nslices = (n + kSellC - 1) / kSellC;
+    int32_t* deg = nullptr;
+    GBK_CUDA(cudaMalloc(&deg, sizeof(int32_t) * (n > 0 ? n : 1)));
+    GBK_CUDA(cudaMalloc(&f->perm, sizeof(int32_t) * (n > 0 ? n : 1)));
+    if (n > 0) {
+        k_degrees<<<blocks_for(n), 256, 0, s>>>(a.ptr, n, deg);
+        GBK_LAUNCHED();
+    }
+    if (sigma > 1 && n > 1) {
+        unsigned long long *keys = nullptr, *keys2 = nullptr;
+        int32_t* ids = nullptr;
+        GBK_CUDA(cudaMalloc(&keys, sizeof(unsigned long long) * n));
+        GBK_CUDA(cudaMalloc(&keys2, sizeof(unsigned long long) * n));
+        GBK_CUDA(cudaMalloc(&ids, sizeof(int32_t) * n));
+        k_sigma_keys<<<blocks_for(n), 256, 0, s>>>(deg, n, sigma, keys, ids);
+        GBK_LAUNCHED();
+        size_t tb = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, ids, f->perm, (int)n, 0, 64, s);
+        void* tmp = nullptr;
+        GBK_CUDA(cudaMalloc(&tmp, tb));
+        GBK_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, ids, f->perm, (int)n, 0, 64, s));
+        count_launch(1);
+        GBK_CUDA(cudaStreamSynchronize(s));
+        cudaFree(tmp);
+        cudaFree(keys);
+        cudaFree(keys2);
+        cudaFree(ids);
+    } else if (n > 0) {
+        k_iota32<<<blocks_for(n), 256, 0, s>>>(f->perm, n);
+        GBK_LAUNCHED();
+    }
+    const int64_t ns = f->nslices;
+    int32_t* is_ov = nullptr;
+    int64_t* stored = nullptr;
+    GBK_CUDA(cudaMalloc(&f->slice_len, sizeof(int32_t) * (ns > 0 ? ns : 1)));
+    GBK_CUDA(cudaMalloc(&f->slice_ptr, sizeof(int64_t) * (ns + 1)));
+    GBK_CUDA(cudaMalloc(&is_ov, sizeof(int32_t) * (ns > 0 ? ns : 1)));
+    GBK_CUDA(cudaMalloc(&stored, sizeof(int64_t) * (ns + 1)));
+    GBK_CUDA(cudaMemsetAsync(stored, 0, sizeof(int64_t) * (ns + 1), s));
+    if (ns > 0) {
+        k_slice_stats<<<blocks_for(ns * 32), 256, 0, s>>>(deg, f->perm, n, ns, f->slice_len, stored, is_ov);
+        GBK_LAUNCHED();
+    }
+    {
+        size_t tb = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tb, stored, f->slice_ptr, (int)(ns + 1), s);
+        void* tmp = nullptr;
+        GBK_CUDA(cudaMalloc(&tmp, tb));
+        GBK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, stored, f->slice_ptr, (int)(ns + 1), s));
+        count_launch(1);
+        GBK_CUDA(cudaMemcpyAsync(&f->padded, f->slice_ptr + ns, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        GBK_CUDA(cudaStreamSynchronize(s));
+        cudaFree(tmp);
+    }
+    GBK_CUDA(cudaMalloc(&f->col, sizeof(int32_t) * (f->padded > 0 ? f->padded : 1)));
+    GBK_CUDA(cudaMalloc(&f->val, sizeof(T) * (f->padded > 0 ? f->padded : 1)));
+    GBK_CUDA(cudaMemsetAsync(f->col, 0xff, sizeof(int32_t) * (f->padded > 0 ? f->padded : 1), s));
+    GBK_CUDA(cudaMemsetAsync(f->val, 0, sizeof(T) * (f->padded > 0 ? f->padded : 1), s));
+    if (n > 0) {
+        k_sell_fill<T><<<blocks_for(n), 256, 0, s>>>(a.ptr, a.idx, (const T*)a.val, f->perm, f->slice_len,
+                                                      f->slice_ptr, n, f->col, (T*)f->val);
+        GBK_LAUNCHED();
+    }
+    // overflow rows
+    if (n > 0) {
+        int32_t *flag = nullptr, *pos = nullptr, *rdeg = nullptr;
+        GBK_CUDA(cudaMalloc(&flag, sizeof(int32_t) * (n + 1)));
+        GBK_CUDA(cudaMalloc(&pos, sizeof(int32_t) * (n + 1)));
+        GBK_CUDA(cudaMemsetAsync(flag + n, 0, sizeof(int32_t), s));
+        k_ov_flags<<<blocks_for(n), 256, 0, s>>>(is_ov, f->perm, n, flag);
+        GBK_LAUNCHED();
+        int rc = cub_scan_excl(flag, pos, n + 1, s);
+        if (rc) return rc;
+        int32_t nov = 0;
+        GBK_CUDA(cudaMemcpyAsync(&nov, pos + n, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        GBK_CUDA(cudaStreamSynchronize(s));
+        f->nov = nov;
+        if (nov > 0) {
+            GBK_CUDA(cudaMalloc(&f->ov_rows, sizeof(int32_t) * nov));
+            GBK_CUDA(cudaMalloc(&rdeg, sizeof(int32_t) * (nov + 1)));
+            GBK_CUDA(cudaMemsetAsync(rdeg + nov, 0, sizeof(int32_t), s));
+            k_ov_compact<<<blocks_for(n), 256, 0, s>>>(flag, pos, f->perm, deg, n, f->ov_rows, rdeg);
+            GBK_LAUNCHED();
+            CsrView& o = f->ov;
+            o.nrows = nov;
+            o.ncols = a.ncols;
+            GBK_CUDA(cudaMalloc(&o.ptr, sizeof(int32_t) * (nov + 1)));
+            rc = cub_scan_excl(rdeg, o.ptr, nov + 1, s);
+            if (rc) return rc;
+            int32_t onnz = 0;
+            GBK_CUDA(cudaMemcpyAsync(&onnz, o.ptr + nov, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            GBK_CUDA(cudaStreamSynchronize(s));
+            o.nnz = onnz;
+            GBK_CUDA(cudaMalloc(&o.idx, sizeof(int32_t) * (onnz > 0 ? onnz : 1)));
+            GBK_CUDA(cudaMalloc(&o.val, sizeof(T) * (onnz > 0 ? onnz : 1)));
+            k_gather_rows<T><<<blocks_for(nov * 32), 256, 0, s>>>(a.ptr, a.idx, (const T*)a.val, f->ov_rows, o.ptr,
+                                                                   nov, o.idx, (T*)o.val);
+            GBK_LAUNCHED();
+            rc = build_tiles(o, sizeof(T), s);
+            if (rc) return rc;
+            GBK_CUDA(cudaMalloc(&f->ov_out, sizeof(T) * nov));
+        }
+        GBK_CUDA(cudaStreamSynchronize(s));
+        cudaFree(flag);
+        cudaFree(pos);
+        cudaFree(rdeg);
+    }
+    cudaFree(is_ov);
+    cudaFree(stored);
+    cudaFree(deg);
+    *out = f;
+    return GBK_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// CSR_SEG / LAV build: col_seg[c] = segment of column c, col_map = optional
+// column renumbering applied to the stored column ids (LAV).
+
+template <typename T>
+int build_segmented(const CsrView& a, const std::vector<int32_t>& col_seg_h, const int32_t* col_map_d,
+                    int32_t nseg, SegCsr* f, cudaStream_t s) {
+    const int64_t n = a.nrows, nnz = a.nnz;
+    f->n = n;
+    f->ncols = a.ncols;
+    f->nsegments = nseg;
+    int32_t* col_seg = nullptr;
+    GBK_CUDA(cudaMalloc(&col_seg, sizeof(int32_t) * (a.ncols > 0 ? a.ncols : 1)));
+    GBK_CUDA(cudaMemcpyAsync(col_seg, col_seg_h.data(), sizeof(int32_t) * a.ncols, cudaMemcpyHostToDevice, s));
+    CsrView& v = f->v;
+    v.ncols = a.ncols;
+    v.nnz = nnz;
+    GBK_CUDA(cudaMalloc(&f->merge_ptr, sizeof(int32_t) * (n + 1)));
+    GBK_CUDA(cudaMemsetAsync(f->merge_ptr, 0, sizeof(int32_t) * (n + 1), s));
+    GBK_CUDA(cudaMalloc(&v.idx, sizeof(int32_t) * (nnz > 0 ? nnz : 1)));
+    GBK_CUDA(cudaMalloc(&v.val, sizeof(T) * (nnz > 0 ? nnz : 1)));
+    if (nnz > 0) {
+        unsigned long long *keys = nullptr, *keys2 = nullptr;
+        int32_t *pos = nullptr, *pos2 = nullptr, *flag = nullptr, *vid = nullptr;
+        GBK_CUDA(cudaMalloc(&keys, 8 * nnz));
+        GBK_CUDA(cudaMalloc(&keys2, 8 * nnz));
+        GBK_CUDA(cudaMalloc(&pos, 4 * nnz));
+        GBK_CUDA(cudaMalloc(&pos2, 4 * nnz));
+        GBK_CUDA(cudaMalloc(&flag, 4 * (nnz + 1)));
+        GBK_CUDA(cudaMalloc(&vid, 4 * (nnz + 1)));
+        k_seg_keys<<<blocks_for(nnz), 256, 0, s>>>(a.ptr, a.idx, n, nnz, col_seg, keys, pos);
+        GBK_LAUNCHED();
+        size_t tb = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, pos, pos2, (int)nnz, 0, 64, s);
+        void* tmp = nullptr;
+        GBK_CUDA(cudaMalloc(&tmp, tb));
+        GBK_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, pos, pos2, (int)nnz, 0, 64, s));
+        count_launch(1);
+        GBK_CUDA(cudaMemsetAsync(flag + nnz, 0, 4, s));
+        k_vrow_flags<<<blocks_for(nnz), 256, 0, s>>>(keys2, nnz, flag);
+        GBK_LAUNCHED();
+        int rc = cub_scan_excl(flag, vid, nnz + 1, s);
+        if (rc) return rc;
+        int32_t nv = 0;
+        GBK_CUDA(cudaMemcpyAsync(&nv, vid + nnz, 4, cudaMemcpyDeviceToHost, s));
+        GBK_CUDA(cudaStreamSynchronize(s));
+        f->nvrows = nv;
+        v.nrows = nv;
+        int32_t *vrow = nullptr, *rowcount = nullptr;
+        GBK_CUDA(cudaMalloc(&v.ptr, 4 * (nv + 1)));
+        GBK_CUDA(cudaMalloc(&vrow, 4 * (nv > 0 ? nv : 1)));
+        GBK_CUDA(cudaMalloc(&rowcount, 4 * (n + 1)));
+        GBK_CUDA(cudaMemsetAsync(rowcount, 0, 4 * (n + 1), s));
+        int32_t nnz32 = (int32_t)nnz;
+        GBK_CUDA(cudaMemcpyAsync(v.ptr + nv, &nnz32, 4, cudaMemcpyHostToDevice, s));
+        k_vrow_build<T><<<blocks_for(nnz), 256, 0, s>>>(keys2, pos2, flag, vid, a.idx, (const T*)a.val, col_map_d,
+                                                         nnz, v.ptr, vrow, v.idx, (T*)v.val, rowcount);
+        GBK_LAUNCHED();
+        rc = cub_scan_excl(rowcount, f->merge_ptr, n + 1, s);
+        if (rc) return rc;
+        GBK_CUDA(cudaMalloc(&f->merge_idx, 4 * (nv > 0 ? nv : 1)));
+        GBK_CUDA(cudaMemsetAsync(rowcount, 0, 4 * (n + 1), s));
+        k_merge_fill<<<blocks_for(nv), 256, 0, s>>>(vrow, nv, f->merge_ptr, rowcount, f->merge_idx);
+        GBK_LAUNCHED();
+        k_merge_sort<<<blocks_for(n), 256, 0, s>>>(f->merge_ptr, n, f->merge_idx);
+        GBK_LAUNCHED();
+        GBK_CUDA(cudaStreamSynchronize(s));
+        cudaFree(tmp);
+        cudaFree(keys);
+        cudaFree(keys2);
+        cudaFree(pos);
+        cudaFree(pos2);
+        cudaFree(flag);
+        cudaFree(vid);
+        cudaFree(vrow);
+        cudaFree(rowcount);
+    } else {
+        v.nrows = 0;
+        GBK_CUDA(cudaMalloc(&v.ptr, 4));
+        GBK_CUDA(cudaMemsetAsync(v.ptr, 0, 4, s));
+        GBK_CUDA(cudaMalloc(&f->merge_idx, 4));
+    }
+    int rc = build_tiles(v, sizeof(T), s);
+    if (rc) return rc;
+    GBK_CUDA(cudaMalloc(&f->partial, sizeof(T) * (f->nvrows > 0 ? f->nvrows : 1)));
+    GBK_CUDA(cudaStreamSynchronize(s));
+    cudaFree(col_seg);
+    return GBK_SUCCESS;
+}
+
+// Column degrees of one orientation, on the host (build-time only).
+int host_col_degrees(const CsrView& a, std::vector<int64_t>& cdeg, cudaStream_t s) {
+    std::vector<int32_t> idx(a.nnz);
+    if (a.nnz) GBK_CUDA(cudaMemcpyAsync(idx.data(), a.idx, 4 * a.nnz, cudaMemcpyDeviceToHost, s));
+    GBK_CUDA(cudaStreamSynchronize(s));
+    cdeg.assign(a.ncols, 0);
+    for (int32_t c : idx) cdeg[c]++;
+    return GBK_SUCCESS;
+}
+
+// CSR_SEG segmentation (seg_csr/build.hpp:34-105): segments of seg_cols
+// columns; the smallest segments, until they hold >= 15 % of nnz, merge into
+// segment 0 (the reference's __CSR_SEG_MERGE_SMALL__ rule).
+template <typename T>
+int build_seg(const CsrView& a, int32_t seg_cols, SegCsr** out, cudaStream_t s) {
+    std::vector<int64_t> cdeg;
+    int rc = host_col_degrees(a, cdeg, s);
+    if (rc) return rc;
+    const int64_t nseg0 = a.ncols > 0 ? (a.ncols - 1) / seg_cols + 1 : 1;
+    std::vector<int64_t> est(nseg0, 0);
+    for (int64_t c = 0; c < a.ncols; c++) est[c / seg_cols] += cdeg[c];
+    std::vector<int64_t> order(nseg0);
+    for (int64_t i = 0; i < nseg0; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return est[x] < est[y]; });
+    std::vector<bool> small(nseg0, false);
+    int64_t merged = 0;
+    for (int64_t i = 0; i < nseg0; i++) {
+        small[order[i]] = true;
+        merged += est[order[i]];
+        if (merged >= (int64_t)(0.15 * a.nnz)) break;
+    }
+    std::vector<int32_t> conv(nseg0);
+    int32_t next = 1;
+    for (int64_t i = 0; i < nseg0; i++) conv[i] = small[i] ? 0 : next++;
+    std::vector<int32_t> col_seg(a.ncols);
+    for (int64_t c = 0; c < a.ncols; c++) col_seg[c] = conv[c / seg_cols];
+    SegCsr* f = new SegCsr();
+    rc = build_segmented<T>(a, col_seg, nullptr, next, f, s);
+    if (rc) return rc;
+    *out = f;
+    return GBK_SUCCESS;
+}
+
+// LAV (lav/build.hpp:97-212): columns renumbered by in-degree, descending;
+// the columns holding the first dense_frac of nnz form "dense" segments of
+// seg_cols columns, the rest one "sparse" segment.
+template <typename T>
+int build_lav(const CsrView& a, int32_t seg_cols, float dense_frac, SegCsr** out, cudaStream_t s) {
+    std::vector<int64_t> cdeg;
+    int rc = host_col_degrees(a, cdeg, s);
+    if (rc) return rc;
+    std::vector<int32_t> new_to_old(a.ncols), old_to_new(a.ncols);
+    for (int64_t c = 0; c < a.ncols; c++) new_to_old[c] = (int32_t)c;
+    std::stable_sort(new_to_old.begin(), new_to_old.end(),
+                     [&](int32_t x, int32_t y) { return cdeg[x] > cdeg[y]; });
+    for (int64_t i = 0; i < a.ncols; i++) old_to_new[new_to_old[i]] = (int32_t)i;
+    int64_t acc = 0, dense_threshold = 0;
+    for (int64_t c = 0; c < a.ncols; c++) {
+        acc += cdeg[new_to_old[c]];
+        if (acc >= (int64_t)(dense_frac * a.nnz)) {
+            dense_threshold = c;
+            break;
+        }
+    }
+    const int32_t ndense = dense_threshold > 0 ? (int32_t)((dense_threshold - 1) / seg_cols + 1) : 0;
+    std::vector<int32_t> col_seg(a.ncols);
+    for (int64_t c = 0; c < a.ncols; c++) {
+        int32_t nc = old_to_new[c];
+        col_seg[c] = nc < dense_threshold ? nc / seg_cols : ndense;
+    }
+    SegCsr* f = new SegCsr();
+    GBK_CUDA(cudaMalloc(&f->col_new_to_old, 4 * (a.ncols > 0 ? a.ncols : 1)));
+    GBK_CUDA(cudaMemcpyAsync(f->col_new_to_old, new_to_old.data(), 4 * a.ncols, cudaMemcpyHostToDevice, s));
+    int32_t* old_to_new_d = nullptr;
+    GBK_CUDA(cudaMalloc(&old_to_new_d, 4 * (a.ncols > 0 ? a.ncols : 1)));
+    GBK_CUDA(cudaMemcpyAsync(old_to_new_d, old_to_new.data(), 4 * a.ncols, cudaMemcpyHostToDevice, s));
+    rc = build_segmented<T>(a, col_seg, old_to_new_d, ndense + 1, f, s);
+    cudaFree(old_to_new_d);
+    if (rc) return rc;
+    GBK_CUDA(cudaMalloc(&f->xr, sizeof(T) * (a.ncols > 0 ? a.ncols : 1)));
+    *out = f;
+    return GBK_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// SpMV dispatch per format
+
+template <int SR, typename T>
+int run_sell(const SellC* f, int accum, const T* x, T* y, cudaStream_t s) {
+    if (f->nslices > 0) {
+        k_sell_spmv<SR, T><<<blocks_for(f->nslices * 32), 256, 0, s>>>(f->slice_len, f->slice_ptr, f->col,
+                                                                       (const T*)f->val, f->perm, f->n, f->nslices,
+                                                                       x, y, accum);
+        GBK_LAUNCHED();
+    }
+    if (f->nov > 0) {
+        int rc = spmv_csr(f->ov, SR, GBK_OP_SECOND, dtype_of_t<T>(), x, f->ov_out, nullptr, 0, 0, s);
+        if (rc) return rc;
+        k_scatter_rows<T><<<blocks_for(f->nov), 256, 0, s>>>(f->ov_rows, (const T*)f->ov_out, f->nov, y, accum);
+        GBK_LAUNCHED();
+    }
+    return GBK_SUCCESS;
+}
+
+template <int SR, typename T>
+int run_seg(const SegCsr* f, int accum, const T* x, T* y, cudaStream_t s) {
+    const T* xin = x;
+    if (f->col_new_to_old) {
+        k_reorder_x<T><<<blocks_for(f->ncols), 256, 0, s>>>(x, f->col_new_to_old, f->ncols, (T*)f->xr);
+        GBK_LAUNCHED();
+        xin = (const T*)f->xr;
+    }
+    if (f->nvrows > 0) {
+        int rc = spmv_csr(f->v, SR, GBK_OP_SECOND, dtype_of_t<T>(), xin, f->partial, nullptr, 0, 0, s);
+        if (rc) return rc;
+    }
+    if (f->n > 0) {
+        k_seg_merge<SR, T><<<blocks_for(f->n), 256, 0, s>>>(f->merge_ptr, f->merge_idx, (const T*)f->partial, f->n,
+                                                            y, accum);
+        GBK_LAUNCHED();
+    }
+    return GBK_SUCCESS;
+}
+
+template <typename T>
+int format_dispatch(gbk_matrix A, int orient, int sr, int accum, const T* x, T* y, cudaStream_t s) {
+#define FMT_CASE(SRV)                                                          \
+    case SRV:                                                                  \
+        if (A->format == GBK_FMT_SELL_C) return run_sell<SRV, T>(A->sell[orient], accum, x, y, s); \
+        if (A->format == GBK_FMT_CSR_SEG) return run_seg<SRV, T>(A->seg[orient], accum, x, y, s);  \
+        return run_seg<SRV, T>(A->lav[orient], accum, x, y, s);
+    switch (sr) {
+        FMT_CASE(GBK_PLUS_TIMES)
+        FMT_CASE(GBK_LOR_LAND)
+        FMT_CASE(GBK_FIRST_MIN)
+        FMT_CASE(GBK_PLUS_SECOND)
+        FMT_CASE(GBK_STRUCTURAL_BOOL)
+        FMT_CASE(GBK_MIN_PLUS)
+        FMT_CASE(GBK_MIN_SECOND)
+        FMT_CASE(GBK_MIN_NOTEQ)
+        FMT_CASE(GBK_PLUS_ONE)
+        default:
+            break;
+    }
+#undef FMT_CASE
+    // non-associative add operators keep the reference's in-order CSR loop
+    const CsrView& v = orient ? A->csc : A->csr;
+    return spmv_csr(v, sr, accum, dtype_of_t<T>(), x, y, nullptr, 0, 0, s);
+}
+
+}  // namespace
+
 int spmv_format(gbk_matrix A, int transpose, int sr, int accum, int dtype, const void* x, void* y,
                 cudaStream_t s) {
-    const CsrView& v = transpose ? A->csc : A->csr;
-    return spmv_csr(v, sr, accum, dtype, x, y, nullptr, 0, 0, s);
+    const int orient = transpose ? 1 : 0;
+    if (dtype == GBK_F32) return format_dispatch<float>(A, orient, sr, accum, (const float*)x, (float*)y, s);
+    return format_dispatch<int32_t>(A, orient, sr, accum, (const int32_t*)x, (int32_t*)y, s);
+}
+
+int free_formats(gbk_matrix A) {
+    for (int o = 0; o < 2; o++) {
+        free_sell(A->sell[o]);
+        free_seg(A->seg[o]);
+        free_seg(A->lav[o]);
+        A->sell[o] = nullptr;
+        A->seg[o] = nullptr;
+        A->lav[o] = nullptr;
+    }
+    A->format = GBK_FMT_CSR;
+    return GBK_SUCCESS;
 }
 
 int build_format(gbk_matrix A, gbk_format fmt, const gbk_format_params* p, cudaStream_t s) {
-    (void)p;
-    (void)s;
-    if (fmt == GBK_FMT_CSR) {
-        A->format = fmt;
-        return GBK_SUCCESS;
+    gbk_format_params prm{};
+    if (p) prm = *p;
+    if (prm.sell_c == 0) prm.sell_c = kSellC;
+    if (prm.sell_sigma == 0) prm.sell_sigma = 4096;
+    if (prm.seg_cols == 0) prm.seg_cols = 131072;
+    if (prm.lav_dense_frac == 0.0f) prm.lav_dense_frac = 0.8f;
+    GBK_REQUIRE(prm.sell_c == kSellC, GBK_UNSUPPORTED, "SELL-C: slice height %d not provided (32 = one warp)",
+                prm.sell_c);
+    GBK_REQUIRE(prm.sell_sigma >= 1 && prm.seg_cols >= 1 && prm.lav_dense_frac > 0.0f && prm.lav_dense_frac <= 1.0f,
+                GBK_INVALID_VALUE, "bad format parameters");
+    free_formats(A);
+    A->params = prm;
+    if (fmt == GBK_FMT_CSR) return GBK_SUCCESS;
+    GBK_REQUIRE(fmt == GBK_FMT_SELL_C || fmt == GBK_FMT_CSR_SEG || fmt == GBK_FMT_LAV, GBK_INVALID_VALUE,
+                "unknown format %d", (int)fmt);
+    int rc = ensure_csc(A, s);
+    if (rc) return rc;
+    for (int o = 0; o < 2; o++) {
+        const CsrView& v = o ? A->csc : A->csr;
+        if (fmt == GBK_FMT_SELL_C) {
+            rc = A->vtype == GBK_F32 ? build_sell<float>(v, prm.sell_sigma, &A->sell[o], s)
+                                     : build_sell<int32_t>(v, prm.sell_sigma, &A->sell[o], s);
+        } else if (fmt == GBK_FMT_CSR_SEG) {
+            rc = A->vtype == GBK_F32 ? build_seg<float>(v, prm.seg_cols, &A->seg[o], s)
+                                     : build_seg<int32_t>(v, prm.seg_cols, &A->seg[o], s);
+        } else {
+            rc = A->vtype == GBK_F32 ? build_lav<float>(v, prm.seg_cols, prm.lav_dense_frac, &A->lav[o], s)
+                                     : build_lav<int32_t>(v, prm.seg_cols, prm.lav_dense_frac, &A->lav[o], s);
+        }
+        if (rc) return rc;
     }
-    set_error("format %d not built yet", (int)fmt);
-    return GBK_UNSUPPORTED;
+    A->format = fmt;
+    return GBK_SUCCESS;
 }
 
-size_t format_bytes(gbk_matrix A) { return 0; }
-int64_t format_padded_nnz(gbk_matrix A) { return A->csr.nnz; }
-int free_formats(gbk_matrix A) { return GBK_SUCCESS; }
+size_t format_bytes(gbk_matrix A) {
+    size_t b = 0;
+    const size_t eb = dtype_size(A->vtype);
+    for (int o = 0; o < 2; o++) {
+        if (A->sell[o]) {
+            const SellC* f = A->sell[o];
+            b += f->padded * (4 + eb) + f->nslices * 12 + f->n * 4 + f->nov * (4 + eb);
+            b += f->ov.nnz * (4 + eb) + (f->ov.nrows + 1) * 4;
+        }
+        const SegCsr* g = A->seg[o] ? A->seg[o] : A->lav[o];
+        if (g) b += g->v.nnz * (4 + eb) + (g->nvrows + 1) * 4 * 2 + (g->n + 1) * 4 + g->nvrows * eb;
+    }
+    return b;
+}
+
+int64_t format_padded_nnz(gbk_matrix A) {
+    if (A->format == GBK_FMT_SELL_C && A->sell[0]) return A->sell[0]->padded + A->sell[0]->ov.nnz;
+    return A->csr.nnz;
+}
 
 }  // namespace gbk
 
