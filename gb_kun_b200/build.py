@@ -30,6 +30,7 @@ CU_SOURCES = [
     "core.cu",
     "matrix.cu",
     "spmv_csr.cu",
+    "spmv_bins.cu",
     "spmv_formats.cu",
     "spmspv.cu",
     "vector_ops.cu",

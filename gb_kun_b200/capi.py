@@ -37,7 +37,7 @@ class GbkError(RuntimeError):
 
 class FormatParams(C.Structure):
     _fields_ = [("sell_c", C.c_int32), ("sell_sigma", C.c_int32), ("seg_cols", C.c_int32),
-                ("lav_dense_frac", C.c_float)]
+                ("lav_dense_frac", C.c_float), ("csr_kernel", C.c_int32)]
 
 
 class MatrixInfo(C.Structure):
@@ -184,8 +184,9 @@ class Matrix:
         check(lib().gbk_matrix_get_info(self.h, C.byref(inf)), "gbk_matrix_get_info")
         return inf
 
-    def set_format(self, fmt: str, sell_c=0, sigma=0, seg_cols=0, lav_frac=0.0, stream=None):
-        p = FormatParams(sell_c, sigma, seg_cols, lav_frac)
+    def set_format(self, fmt: str, sell_c=0, sigma=0, seg_cols=0, lav_frac=0.0, csr_kernel=0, stream=None):
+        """Storage format; csr_kernel picks the CSR kernel (0 default bins, 1 merge-path, 2 bins)."""
+        p = FormatParams(sell_c, sigma, seg_cols, lav_frac, csr_kernel)
         check(lib().gbk_matrix_set_format(self.h, FMT[fmt], C.byref(p), stream_ptr(stream)), "gbk_matrix_set_format")
 
     def arrays(self, transpose=False, stream=None):

@@ -15,8 +15,15 @@ constexpr int kSpmvThreads = 256;
 constexpr int kSpmvItems = 8;
 constexpr int kTileItems = kSpmvThreads * kSpmvItems;
 
+struct RowBins;  // spmv_bins.cu
+
+// CSR kernel choice of a view: degree-binned lane groups or merge-path tiles.
+enum { kKernelAuto = 0, kKernelMerge = 1, kKernelBins = 2 };
+
 struct CsrView {
     int64_t nrows = 0, ncols = 0, nnz = 0;
+    int kernel = kKernelAuto;
+    mutable RowBins* bins = nullptr;  // built on first use
     int32_t* ptr = nullptr;  // nrows + 1
     int32_t* idx = nullptr;  // nnz
     void* val = nullptr;     // nnz of the matrix value type
@@ -50,6 +57,11 @@ struct gbk_matrix_s {
 };
 
 namespace gbk {
+
+int build_bins(const CsrView& v, int elem_bytes, RowBins** out, cudaStream_t s);
+void free_bins(RowBins* b);
+int spmv_binned(const RowBins* rb, const CsrView& v, int sr, int accum, int dtype, const void* x, void* y,
+                const void* mask, int mdt, int mmode, cudaStream_t s);
 
 int ensure_csc(gbk_matrix A, cudaStream_t s);
 int build_tiles(CsrView& v, int elem_bytes, cudaStream_t s);

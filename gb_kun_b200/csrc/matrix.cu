@@ -97,6 +97,7 @@ void free_view(CsrView& v) {
     cudaFree(v.carry_row);
     cudaFree(v.carry_val);
     cudaFree(v.head_val);
+    free_bins(v.bins);
     v = CsrView{};
 }
 
@@ -149,6 +150,7 @@ int ensure_csc(gbk_matrix A, cudaStream_t s) {
     }
     int rc = build_tiles(t, (int)eb, s);
     if (rc) return rc;
+    t.kernel = A->params.csr_kernel;
     A->has_csc = true;
     return GBK_SUCCESS;
 }

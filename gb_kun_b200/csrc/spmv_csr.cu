@@ -253,8 +253,19 @@ int dispatch(const CsrView& v, int sr, int accum, const void* x, void* y, const 
 
 }  // namespace
 
+static bool assoc_semiring(int sr) { return sr != GBK_FIRST_WINS && sr != GBK_CUSTOM_LESS_PLUS; }
+
 int spmv_csr(const CsrView& v, int sr, int accum, int dtype, const void* x, void* y, const void* mask,
              int mask_dtype, int mask_mode, cudaStream_t s) {
+    GBK_REQUIRE(dtype == GBK_F32 || dtype == GBK_I32, GBK_UNSUPPORTED,
+                "spmv: element type %d unsupported (GBK_F32 or GBK_I32)", dtype);
+    if (v.kernel != kKernelMerge && assoc_semiring(sr) && v.nrows > 0) {
+        if (!v.bins) {
+            int rc = build_bins(v, (int)dtype_size(dtype), &v.bins, s);
+            if (rc) return rc;
+        }
+        return spmv_binned(v.bins, v, sr, accum, dtype, x, y, mask, mask_dtype, mask_mode, s);
+    }
     if (dtype == GBK_F32) return dispatch<float>(v, sr, accum, x, y, mask, mask_dtype, mask_mode, s);
     if (dtype == GBK_I32) return dispatch<int32_t>(v, sr, accum, x, y, mask, mask_dtype, mask_mode, s);
     set_error("spmv: element type %d unsupported (GBK_F32 or GBK_I32)", dtype);

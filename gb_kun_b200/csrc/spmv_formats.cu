@@ -742,8 +742,12 @@ int build_format(gbk_matrix A, gbk_format fmt, const gbk_format_params* p, cudaS
                 prm.sell_c);
     GBK_REQUIRE(prm.sell_sigma >= 1 && prm.seg_cols >= 1 && prm.lav_dense_frac > 0.0f && prm.lav_dense_frac <= 1.0f,
                 GBK_INVALID_VALUE, "bad format parameters");
+    GBK_REQUIRE(prm.csr_kernel >= 0 && prm.csr_kernel <= kKernelBins, GBK_INVALID_VALUE, "bad csr_kernel %d",
+                prm.csr_kernel);
     free_formats(A);
     A->params = prm;
+    A->csr.kernel = prm.csr_kernel;
+    A->csc.kernel = prm.csr_kernel;
     if (fmt == GBK_FMT_CSR) return GBK_SUCCESS;
     GBK_REQUIRE(fmt == GBK_FMT_SELL_C || fmt == GBK_FMT_CSR_SEG || fmt == GBK_FMT_LAV, GBK_INVALID_VALUE,
                 "unknown format %d", (int)fmt);

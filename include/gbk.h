@@ -33,6 +33,7 @@ typedef struct gbk_format_params {
     int32_t sell_sigma;      /* SELL-C sorting window in rows; default 4096; 1 = no sort */
     int32_t seg_cols;        /* CSR_SEG / LAV column-segment width; default 131072 (512 KiB of f32 x) */
     float lav_dense_frac;    /* LAV: fraction of nnz in the dense column segments; default 0.8 */
+    int32_t csr_kernel;      /* CSR kernel: 0 default (degree bins), 1 merge-path tiles, 2 degree bins */
 } gbk_format_params;
 
 /* A mask argument: either dense (n entries of `dtype`, non-zero = set) or

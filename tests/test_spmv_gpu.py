@@ -38,12 +38,17 @@ def dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
+KERNELS = [1, 2]  # merge-path tiles, degree bins
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("gi", range(6))
-def test_plus_times_f32_vs_fp64(capi, oracle, gi):
+def test_plus_times_f32_vs_fp64(capi, oracle, gi, kernel):
     g = list(graphs())[gi]
     val = gg.values_f32(g, seed=7)
     x = gg.vector_f32(g.n, seed=8)
     A = capi.Matrix.from_graph(g, val)
+    A.set_format("CSR", csr_kernel=kernel)
     y = torch.full((g.n,), 7.0, device="cuda")
     A.mxv(dev(x), y)
     ref = oracle.spmv_f64(g, val, x)
@@ -56,9 +61,10 @@ SEMIRINGS_EXACT = ["lor_land", "min_plus", "min_second", "min_noteq", "first_min
                    "first_wins", "custom_less_plus"]
 
 
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("sr", SEMIRINGS_EXACT + ["plus_one"])
 @pytest.mark.parametrize("dtype", ["f32", "i32"])
-def test_semirings_exact(capi, oracle, sr, dtype):
+def test_semirings_exact(capi, oracle, sr, dtype, kernel):
     for g in list(graphs())[:4]:
         if dtype == "f32":
             val = gg.values_f32(g, seed=11)
@@ -69,6 +75,7 @@ def test_semirings_exact(capi, oracle, sr, dtype):
             x = (gg.vector_f32(g.n, seed=12) * 50).astype(np.int32)
             x[::5] = np.iinfo(np.int32).max
         A = capi.Matrix.from_graph(g, val)
+        A.set_format("CSR", csr_kernel=kernel)
         y0 = np.ones(g.n, val.dtype)
         y = dev(y0)
         A.mxv(dev(x), y, semiring=sr)
@@ -90,9 +97,10 @@ def test_accumulators(capi, oracle, accum):
     assert np.array_equal(y.cpu().numpy(), expect)
 
 
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("mode", ["default", "structure", "str_comp", "comp", "scmp"])
 @pytest.mark.parametrize("mdtype", ["bool", "f32", "i64"])
-def test_dense_mask(capi, oracle, mode, mdtype):
+def test_dense_mask(capi, oracle, mode, mdtype, kernel):
     from gb_kun_b200.capi import MASK
     g = gg.rmat(12, 8, seed=31, undirected=True)
     val = np.ones(g.nnz, np.float32)
@@ -101,6 +109,7 @@ def test_dense_mask(capi, oracle, mode, mdtype):
     mask = {"bool": m.astype(np.bool_), "f32": m.astype(np.float32), "i64": m.astype(np.int64)}[mdtype]
     y0 = np.full(g.n, 3.0, np.float32)
     A = capi.Matrix.from_graph(g, val)
+    A.set_format("CSR", csr_kernel=kernel)
     y = dev(y0)
     A.mxv(dev(x), y, semiring="lor_land", mask=dev(mask), mask_mode=mode)
     expect = oracle.mxv("lor_land", g, val, x, y0, mask=mask, mask_mode=MASK[mode])
