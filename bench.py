@@ -37,6 +37,10 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "SpMV GB/s (% HBM peak) & GTEPS; served-query QPS + p50/p99 vs plain GPU"
 FALLBACK_HBM_GBS = 6650.0
+# Format the reference CPU code runs in: "auto" maps to CSR_SEG, the
+# reference's fastest format in its own SpMV measurements.
+REF_FORMAT = {"auto": 3, "CSR": 0, "SELL_C": 6, "CSR_SEG": 3, "LAV": 4}
+REF_FORMAT_NAME = {0: "CSR", 3: "CSR_SEG", 4: "LAV", 6: "SELL_C"}
 
 
 def parse():
@@ -50,7 +54,8 @@ def parse():
     p.add_argument("--scale", type=int, default=22)
     p.add_argument("--edge-factor", type=int, default=16)
     p.add_argument("--graph", default="rmat", choices=["rmat", "er"])
-    p.add_argument("--format", default="CSR", choices=["CSR", "SELL_C", "CSR_SEG", "LAV"])
+    p.add_argument("--format", default="auto", choices=["auto", "CSR", "SELL_C", "CSR_SEG", "LAV"],
+                   help="storage format; auto = the per-graph autotuner's choice")
     p.add_argument("--seed", type=int, default=42)
     p.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -178,14 +183,14 @@ def cpu_baseline(args, g, val, x):
         if not Reference.available():
             return None
         R = Reference()
-        fmt = {"CSR": 0, "SELL_C": 6, "CSR_SEG": 3, "LAV": 4}[args.format]
+        fmt = REF_FORMAT[args.format]
         _, ms = R.spmv(g, val, x, fmt=fmt, semiring=0, warmup=1, reps=1)
         reps = max(3, min(200, int(args.cpu_baseline_seconds * 1000 / max(ms, 1e-3))))
         _, ms = R.spmv(g, val, x, fmt=fmt, semiring=0, warmup=0, reps=reps)
         return {"value": alg_bytes(g) / (ms * 1e-3) / 1e9, "unit": "GB/s", "cores": R.max_threads(),
                 "kind": "reference",
                 "sample": f"full matrix, median of {reps} GrB_mxv calls (reference CPU code, "
-                          f"{args.format}, OMP_NUM_THREADS={R.max_threads()})",
+                          f"format {REF_FORMAT_NAME[fmt]}, OMP_NUM_THREADS={R.max_threads()})",
                 "ms_per_spmv": ms}
     except Exception as e:  # reported, never fatal for the GPU number
         return {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
@@ -267,7 +272,10 @@ def run_ours(args):
     capi.init(local)
     g, val, x = make_input(args)
     A = capi.Matrix.from_graph(g, val)
-    if args.format != "CSR":
+    tuned = None
+    if args.format == "auto":
+        tuned = A.autotune(reps=20).describe()
+    else:
         A.set_format(args.format)
     stream = torch.cuda.current_stream()
     dx = torch.from_numpy(x).cuda()
@@ -333,6 +341,8 @@ def run_ours(args):
     value = world * B / (ms_per_step * 1e-3) / 1e9
     cfg = workload_config(args, g)
     cfg["parallelism"] = f"replicas{world}" if world > 1 else "single"
+    if tuned:
+        cfg["format"] = tuned
     out = {
         "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5), "higher_is_better": True, "scaling": "weak",
@@ -376,7 +386,7 @@ def run_reference(args):
         return
     g, val, x = make_input(args)
     R = Reference()
-    fmt = {"CSR": 0, "SELL_C": 6, "CSR_SEG": 3, "LAV": 4}[args.format]
+    fmt = REF_FORMAT[args.format]
     steps = max(1, min(args.steps, 20))
     warm = max(1, min(args.warmup, 3))
     _, ms = R.spmv(g, val, x, fmt=fmt, semiring=0, warmup=warm, reps=steps)

@@ -35,6 +35,7 @@ CU_SOURCES = [
     "spmspv.cu",
     "vector_ops.cu",
     "spgemm.cu",
+    "tune.cu",
     "batched.cu",
 ]
 

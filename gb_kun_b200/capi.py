@@ -46,6 +46,24 @@ class MatrixInfo(C.Structure):
                 ("ntiles", C.c_int64), ("has_csc", C.c_int32)]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("format", C.c_int32), ("sell_sigma", C.c_int32), ("csr_kernel", C.c_int32), ("cached", C.c_int32),
+                ("ncandidates", C.c_int32), ("best_ms", C.c_float), ("candidate_ms", C.c_float * 8)]
+
+    CANDIDATES = ["CSR_bins", "CSR_merge", "SELL_C_s1", "SELL_C_s256", "SELL_C_s4096", "CSR_SEG", "LAV"]
+
+    def describe(self) -> dict:
+        names = {0: "CSR", 3: "CSR_SEG", 4: "LAV", 6: "SELL_C"}
+        d = {"format": names.get(self.format, str(self.format)), "cached": bool(self.cached)}
+        if self.format == 6:
+            d["sigma"] = self.sell_sigma
+        if self.format == 0:
+            d["csr_kernel"] = {1: "merge-path", 2: "degree-bins"}.get(self.csr_kernel, "default")
+        if not self.cached:
+            d["candidate_ms"] = {n: round(self.candidate_ms[i], 4) for i, n in enumerate(self.CANDIDATES)}
+        return d
+
+
 class Mask(C.Structure):
     """gbk_mask: dense (dense != NULL) or sparse (ids, nvals) mask argument."""
     _fields_ = [("dense", C.c_void_p), ("dtype", C.c_int32), ("mode", C.c_int32), ("ids", C.c_void_p),
@@ -62,6 +80,7 @@ def _declare(lib):
         "gbk_mxv_sparse_mask": ([vp, ci, ci, ci, ci, vp, vp, vp, i64, ci, vp], ci),
         "gbk_spmspv": ([vp, ci, ci, ci, ci, vp, vp, i64, vp, mp, vp], ci),
         "gbk_mxm_masked": ([C.POINTER(vp), vp, vp, vp, ci, ci, vp], ci),
+        "gbk_matrix_autotune": ([vp, ci, ci, i32, C.POINTER(TuneResult), vp], ci),
         "gbk_vec_nvals": ([vp, ci, i64, C.POINTER(i64), vp], ci),
         "gbk_vec_to_sparse": ([vp, ci, i64, vp, vp, C.POINTER(i64), vp], ci),
         "gbk_vec_to_dense": ([vp, vp, i64, ci, vp, i64, vp], ci),
@@ -188,6 +207,13 @@ class Matrix:
         """Storage format; csr_kernel picks the CSR kernel (0 default bins, 1 merge-path, 2 bins)."""
         p = FormatParams(sell_c, sigma, seg_cols, lav_frac, csr_kernel)
         check(lib().gbk_matrix_set_format(self.h, FMT[fmt], C.byref(p), stream_ptr(stream)), "gbk_matrix_set_format")
+
+    def autotune(self, transpose=False, semiring="plus_times", reps=20, stream=None) -> TuneResult:
+        """Time every format / kernel candidate and keep the fastest on this matrix."""
+        r = TuneResult()
+        check(lib().gbk_matrix_autotune(self.h, int(transpose), SEMIRING[semiring], reps, C.byref(r),
+                                        stream_ptr(stream)), "gbk_matrix_autotune")
+        return r
 
     def arrays(self, transpose=False, stream=None):
         p, i, v = C.c_void_p(), C.c_void_p(), C.c_void_p()

@@ -56,6 +56,25 @@ template <typename T>
 __device__ __forceinline__ T ld_stream(const T* p) {
     return __ldcs(p);
 }
+
+// L2 eviction policies created per use (createpolicy, PTX ISA 7.4+): the
+// gathered vector x is marked evict-last so the matrix stream does not push
+// it out of L2.  An instruction-level hint: no device setting is changed.
+__device__ __forceinline__ uint64_t policy_evict_last() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ float ld_keep(const float* p, uint64_t pol) {
+    float v;
+    asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int32_t ld_keep(const int32_t* p, uint64_t pol) {
+    int32_t v;
+    asm volatile("ld.global.nc.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
 // Re-used across CTAs (x gathers): read-only path, kept in L2.
 template <typename T>
 __device__ __forceinline__ T ld_reuse(const T* p) {

@@ -76,8 +76,10 @@ __device__ __forceinline__ void rows_by_group(const BinTable& bt, int bin, int l
         r = perm[bt.item_start[bin] + k];
         if (mask && !mask_selects(mask, mdt, mmode, r)) skip = true;
         if (!skip) {
+            const uint64_t pol = policy_evict_last();
             const int32_t b = ld_stream(ptr + r), e = ld_stream(ptr + r + 1);
-            for (int32_t q = b + sub; q < e; q += G) acc = S::add(acc, S::mul(ld_stream(val + q), ld_reuse(x + ld_stream(idx + q))));
+            for (int32_t q = b + sub; q < e; q += G)
+                acc = S::add(acc, S::mul(ld_stream(val + q), ld_keep(x + ld_stream(idx + q), pol)));
         }
     }
     if (G > 1) {
@@ -96,6 +98,7 @@ template <int SR, typename T>
 __device__ __forceinline__ T warp_range(int32_t b, int32_t e, const int32_t* __restrict__ idx,
                                         const T* __restrict__ val, const T* __restrict__ x, int lane) {
     using S = Semiring<SR, T>;
+    const uint64_t pol = policy_evict_last();
     T acc = S::identity();
     int32_t q = b + lane;
     for (; q + 96 < e; q += 128) {
@@ -103,12 +106,12 @@ __device__ __forceinline__ T warp_range(int32_t b, int32_t e, const int32_t* __r
                       c3 = ld_stream(idx + q + 96);
         const T a0 = ld_stream(val + q), a1 = ld_stream(val + q + 32), a2 = ld_stream(val + q + 64),
                 a3 = ld_stream(val + q + 96);
-        acc = S::add(acc, S::mul(a0, ld_reuse(x + c0)));
-        acc = S::add(acc, S::mul(a1, ld_reuse(x + c1)));
-        acc = S::add(acc, S::mul(a2, ld_reuse(x + c2)));
-        acc = S::add(acc, S::mul(a3, ld_reuse(x + c3)));
+        acc = S::add(acc, S::mul(a0, ld_keep(x + c0, pol)));
+        acc = S::add(acc, S::mul(a1, ld_keep(x + c1, pol)));
+        acc = S::add(acc, S::mul(a2, ld_keep(x + c2, pol)));
+        acc = S::add(acc, S::mul(a3, ld_keep(x + c3, pol)));
     }
-    for (; q < e; q += 32) acc = S::add(acc, S::mul(ld_stream(val + q), ld_reuse(x + ld_stream(idx + q))));
+    for (; q < e; q += 32) acc = S::add(acc, S::mul(ld_stream(val + q), ld_keep(x + ld_stream(idx + q), pol)));
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) acc = S::add(acc, __shfl_xor_sync(0xffffffffu, acc, off));
     return acc;

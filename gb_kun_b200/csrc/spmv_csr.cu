@@ -75,10 +75,11 @@ __global__ void __launch_bounds__(kSpmvThreads) k_spmv_merge(
                 a[i] = ld_stream(val + nz0 + k);
             }
         }
+        const uint64_t pol = policy_evict_last();
 #pragma unroll
         for (int i = 0; i < kSpmvItems; i++) {
             int k = tid + i * kSpmvThreads;
-            if (k < nnzt) s_prod[k] = S::mul(a[i], ld_reuse(x + c[i]));
+            if (k < nnzt) s_prod[k] = S::mul(a[i], ld_keep(x + c[i], pol));
         }
     }
     __syncthreads();

@@ -88,6 +88,7 @@ __global__ void __launch_bounds__(256) k_sell_spmv(const int32_t* __restrict__ s
     const int len = slice_len[s];
     if (len < 0) return;  // overflow slice: computed from the overflow CSR
     const int64_t base = slice_ptr[s] + lane;
+    const uint64_t pol = policy_evict_last();
     T acc = S::identity();
     int j = 0;
     for (; j + 4 <= len; j += 4) {
@@ -99,11 +100,11 @@ __global__ void __launch_bounds__(256) k_sell_spmv(const int32_t* __restrict__ s
         for (int u = 0; u < 4; u++) a[u] = ld_stream(val + base + (int64_t)(j + u) * kSellC);
 #pragma unroll
         for (int u = 0; u < 4; u++)
-            if (c[u] >= 0) acc = S::add(acc, S::mul(a[u], ld_reuse(x + c[u])));
+            if (c[u] >= 0) acc = S::add(acc, S::mul(a[u], ld_keep(x + c[u], pol)));
     }
     for (; j < len; j++) {
         int c = ld_stream(col + base + (int64_t)j * kSellC);
-        if (c >= 0) acc = S::add(acc, S::mul(ld_stream(val + base + (int64_t)j * kSellC), ld_reuse(x + c)));
+        if (c >= 0) acc = S::add(acc, S::mul(ld_stream(val + base + (int64_t)j * kSellC), ld_keep(x + c, pol)));
     }
     const int64_t p = s * kSellC + lane;
     if (p < n) {

@@ -86,6 +86,25 @@ int gbk_matrix_csr_arrays(gbk_matrix A, int transpose, const int32_t** ptr, cons
  * GBK_FMT_CSR drops any optimised format. */
 int gbk_matrix_set_format(gbk_matrix A, gbk_format fmt, const gbk_format_params* params, void* stream);
 
+typedef struct gbk_tune_result {
+    int32_t format;          /* chosen gbk_format */
+    int32_t sell_sigma;      /* chosen SELL-C window (SELL-C only) */
+    int32_t csr_kernel;      /* chosen CSR kernel (CSR only) */
+    int32_t cached;          /* 1 when the choice came from the cache (nothing was timed) */
+    int32_t ncandidates;
+    float best_ms;
+    float candidate_ms[8];   /* CSR bins, CSR merge-path, SELL-C sigma 1 / 256 / 4096, CSR_SEG, LAV */
+} gbk_tune_result;
+
+/* Per-graph autotuner (no counterpart in the reference, which takes the
+ * format from its -format flag, src/helpers/cmd_parser/cmd_parser.hpp, and
+ * fixes C / sigma at compile time, src/backend/la_backend.h:16-34): times
+ * `reps` unmasked SpMVs of every candidate format / kernel for the given
+ * orientation and semiring, keeps the fastest on A, and caches the choice by
+ * graph fingerprint (process-wide, plus the file GBK_TUNE_CACHE if set). */
+int gbk_matrix_autotune(gbk_matrix A, int transpose, gbk_semiring sr, int32_t reps, gbk_tune_result* result,
+                        void* stream);
+
 /* ---- SpMV / SpMSpV ------------------------------------------------------ */
 
 /* y = accum(y, A (+.x) x) over a semiring, every operand of type `dtype`

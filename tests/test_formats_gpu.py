@@ -88,6 +88,23 @@ def test_sell_padding_accounting(capi):
     assert A.info().padded_nnz >= g.nnz
 
 
+def test_autotune_picks_a_correct_format_and_caches(capi, oracle):
+    g = GRAPHS["rmat13"]()
+    val = gg.values_f32(g, seed=7)
+    x = gg.vector_f32(g.n, seed=8)
+    A = capi.Matrix.from_graph(g, val)
+    r1 = A.autotune(reps=3)
+    assert r1.cached == 0 and r1.best_ms > 0
+    assert all(r1.candidate_ms[i] > 0 for i in range(r1.ncandidates))
+    y = torch.zeros(g.n, device="cuda")
+    A.mxv(dev(x), y)
+    assert rel_l1(y.cpu().numpy(), oracle.spmv_f64(g, val, x)) < REL_L1_TOL
+    B = capi.Matrix.from_graph(g, val)  # same graph: the choice comes from the cache
+    r2 = B.autotune(reps=3)
+    assert r2.cached == 1 and r2.format == r1.format and r2.sell_sigma == r1.sell_sigma
+    assert B.info().format == r1.format
+
+
 def test_masked_call_uses_csr_semantics(capi, oracle):
     """Masked SpMV always runs the CSR kernel, as the reference's SpMV does."""
     g = GRAPHS["rmat12u"]()
