@@ -98,20 +98,38 @@ template <int SR, typename T>
 __device__ __forceinline__ T warp_range(int32_t b, int32_t e, const int32_t* __restrict__ idx,
                                         const T* __restrict__ val, const T* __restrict__ x, int lane) {
     using S = Semiring<SR, T>;
+    // software-pipelined: the next U groups of 32 entries are loaded before
+    // the x values of the current groups are gathered
+    constexpr int U = 4;
     const uint64_t pol = policy_evict_last();
     T acc = S::identity();
+    int c[U];
+    T a[U];
     int32_t q = b + lane;
-    for (; q + 96 < e; q += 128) {
-        const int32_t c0 = ld_stream(idx + q), c1 = ld_stream(idx + q + 32), c2 = ld_stream(idx + q + 64),
-                      c3 = ld_stream(idx + q + 96);
-        const T a0 = ld_stream(val + q), a1 = ld_stream(val + q + 32), a2 = ld_stream(val + q + 64),
-                a3 = ld_stream(val + q + 96);
-        acc = S::add(acc, S::mul(a0, ld_keep(x + c0, pol)));
-        acc = S::add(acc, S::mul(a1, ld_keep(x + c1, pol)));
-        acc = S::add(acc, S::mul(a2, ld_keep(x + c2, pol)));
-        acc = S::add(acc, S::mul(a3, ld_keep(x + c3, pol)));
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        const int32_t p = q + 32 * u;
+        c[u] = p < e ? ld_stream(idx + p) : -1;
+        a[u] = p < e ? ld_stream(val + p) : T(0);
     }
-    for (; q < e; q += 32) acc = S::add(acc, S::mul(ld_stream(val + q), ld_keep(x + ld_stream(idx + q), pol)));
+    for (; q < e; q += 32 * U) {
+        int cn[U];
+        T an[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int32_t p = q + 32 * (U + u);
+            cn[u] = p < e ? ld_stream(idx + p) : -1;
+            an[u] = p < e ? ld_stream(val + p) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (c[u] >= 0) acc = S::add(acc, S::mul(a[u], ld_keep(x + c[u], pol)));
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            c[u] = cn[u];
+            a[u] = an[u];
+        }
+    }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) acc = S::add(acc, __shfl_xor_sync(0xffffffffu, acc, off));
     return acc;

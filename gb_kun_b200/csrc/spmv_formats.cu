@@ -33,7 +33,9 @@
 namespace gbk {
 
 constexpr int kSellC = 32;
-constexpr int kSellMaxLen = 256;
+constexpr int kSellMaxLen = 1 << 30;  // long slices are cut into work items instead
+constexpr int kSellChunk = 64;        // slice steps per work item (one warp)
+constexpr int kSellUnroll = 8;        // steps per pipelined load group
 
 struct SellC {
     int64_t n = 0;           // rows
@@ -50,6 +52,14 @@ struct SellC {
     int32_t* ov_rows = nullptr;   // original row ids
     CsrView ov;                   // rows 0..nov-1 of the overflow CSR
     void* ov_out = nullptr;       // nov partial results
+    // warp work items: kSellChunk steps of one slice each
+    int64_t nitems = 0;
+    int32_t* item_slice = nullptr;
+    int32_t* item_j0 = nullptr;
+    int32_t* slice_item0 = nullptr;  // nslices + 1
+    void* item_out = nullptr;        // 32 partials per item of a multi-item slice
+    int64_t nmulti = 0;
+    int32_t* multi = nullptr;        // slices with more than one item
 };
 
 struct SegCsr {
@@ -75,42 +85,111 @@ inline unsigned blocks_for(int64_t work, int threads = 256) {
 // ---------------------------------------------------------------------------
 // SELL-C kernels
 
+// One warp per work item: steps [j0, j0 + kSellChunk) of one slice.  The loop
+// is software-pipelined: the col / val group of the next kSellUnroll steps is
+// loaded before the x values of the current group are gathered, so two
+// dependent memory round trips overlap.  A slice cut into several items
+// leaves per-item partials that k_sell_fold combines in item order.
 template <int SR, typename T>
-__global__ void __launch_bounds__(256) k_sell_spmv(const int32_t* __restrict__ slice_len,
-                                                   const int64_t* __restrict__ slice_ptr,
-                                                   const int32_t* __restrict__ col, const T* __restrict__ val,
-                                                   const int32_t* __restrict__ perm, int64_t n, int64_t nslices,
-                                                   const T* __restrict__ x, T* __restrict__ y, int accum) {
+__global__ void __launch_bounds__(256) k_sell_items(const int32_t* __restrict__ item_slice,
+                                                    const int32_t* __restrict__ item_j0,
+                                                    const int32_t* __restrict__ slice_item0,
+                                                    const int32_t* __restrict__ slice_len,
+                                                    const int64_t* __restrict__ slice_ptr,
+                                                    const int32_t* __restrict__ col, const T* __restrict__ val,
+                                                    const int32_t* __restrict__ perm, int64_t n, int64_t nitems,
+                                                    const T* __restrict__ x, T* __restrict__ y, int accum,
+                                                    T* __restrict__ item_out) {
     using S = Semiring<SR, T>;
+    constexpr int U = kSellUnroll;
     const int lane = threadIdx.x & 31;
-    const int64_t s = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (s >= nslices) return;
-    const int len = slice_len[s];
-    if (len < 0) return;  // overflow slice: computed from the overflow CSR
+    const int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (k >= nitems) return;
+    const int32_t s = item_slice[k];
+    const int32_t j0 = item_j0[k];
+    const int32_t j1 = min(j0 + kSellChunk, slice_len[s]);
     const int64_t base = slice_ptr[s] + lane;
     const uint64_t pol = policy_evict_last();
     T acc = S::identity();
-    int j = 0;
-    for (; j + 4 <= len; j += 4) {
-        int c[4];
-        T a[4];
+    int c[U];
+    T a[U];
 #pragma unroll
-        for (int u = 0; u < 4; u++) c[u] = ld_stream(col + base + (int64_t)(j + u) * kSellC);
+    for (int u = 0; u < U; u++) {
+        const bool in = j0 + u < j1;
+        c[u] = in ? ld_stream(col + base + (int64_t)(j0 + u) * kSellC) : -1;
+        a[u] = in ? ld_stream(val + base + (int64_t)(j0 + u) * kSellC) : T(0);
+    }
+    for (int j = j0; j < j1; j += U) {
+        int cn[U];
+        T an[U];
+        const int jn = j + U;
 #pragma unroll
-        for (int u = 0; u < 4; u++) a[u] = ld_stream(val + base + (int64_t)(j + u) * kSellC);
+        for (int u = 0; u < U; u++) {
+            const bool in = jn + u < j1;
+            cn[u] = in ? ld_stream(col + base + (int64_t)(jn + u) * kSellC) : -1;
+            an[u] = in ? ld_stream(val + base + (int64_t)(jn + u) * kSellC) : T(0);
+        }
 #pragma unroll
-        for (int u = 0; u < 4; u++)
+        for (int u = 0; u < U; u++)
             if (c[u] >= 0) acc = S::add(acc, S::mul(a[u], ld_keep(x + c[u], pol)));
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            c[u] = cn[u];
+            a[u] = an[u];
+        }
     }
-    for (; j < len; j++) {
-        int c = ld_stream(col + base + (int64_t)j * kSellC);
-        if (c >= 0) acc = S::add(acc, S::mul(ld_stream(val + base + (int64_t)j * kSellC), ld_keep(x + c, pol)));
+    if (slice_item0[s + 1] - slice_item0[s] == 1) {
+        const int64_t p = (int64_t)s * kSellC + lane;
+        if (p < n) {
+            const int32_t r = perm[p];
+            y[r] = (accum == GBK_OP_SECOND) ? acc : binop<T>(accum, y[r], acc);
+        }
+    } else {
+        item_out[k * kSellC + lane] = acc;
     }
-    const int64_t p = s * kSellC + lane;
+}
+
+// Slices cut into several items: fold the partials of each lane in item order.
+template <int SR, typename T>
+__global__ void k_sell_fold(const int32_t* __restrict__ multi, int64_t nmulti, const int32_t* __restrict__ slice_item0,
+                            const T* __restrict__ item_out, const int32_t* __restrict__ perm, int64_t n,
+                            T* __restrict__ y, int accum) {
+    using S = Semiring<SR, T>;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= nmulti * kSellC) return;
+    const int32_t s = multi[t / kSellC];
+    const int lane = (int)(t % kSellC);
+    T acc = S::identity();
+    for (int32_t k = slice_item0[s]; k < slice_item0[s + 1]; k++) acc = S::add(acc, item_out[(int64_t)k * kSellC + lane]);
+    const int64_t p = (int64_t)s * kSellC + lane;
     if (p < n) {
         const int32_t r = perm[p];
         y[r] = (accum == GBK_OP_SECOND) ? acc : binop<T>(accum, y[r], acc);
     }
+}
+
+// Work items of a slice: ceil(len / kSellChunk), at least 1 (empty slices
+// still write their rows); overflow slices have none.
+__global__ void k_sell_item_counts(const int32_t* len, int64_t ns, int32_t* cnt) {
+    int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s < ns) cnt[s] = len[s] < 0 ? 0 : max(1, (len[s] + kSellChunk - 1) / kSellChunk);
+    if (s == ns) cnt[s] = 0;
+}
+
+__global__ void k_sell_item_fill(const int32_t* cnt, const int32_t* first, int64_t ns, int32_t* item_slice,
+                                 int32_t* item_j0, int32_t* multi_flag) {
+    int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s >= ns) return;
+    for (int32_t c = 0; c < cnt[s]; c++) {
+        item_slice[first[s] + c] = (int32_t)s;
+        item_j0[first[s] + c] = c * kSellChunk;
+    }
+    multi_flag[s] = cnt[s] > 1 ? 1 : 0;
+}
+
+__global__ void k_compact_flags(const int32_t* flag, const int32_t* pos, int64_t n, int32_t* out) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n && flag[i]) out[pos[i]] = (int32_t)i;
 }
 
 template <typename T>
@@ -330,6 +409,11 @@ int free_sell(SellC* f) {
     cudaFree(f->val);
     cudaFree(f->ov_rows);
     cudaFree(f->ov_out);
+    cudaFree(f->item_slice);
+    cudaFree(f->item_j0);
+    cudaFree(f->slice_item0);
+    cudaFree(f->item_out);
+    cudaFree(f->multi);
     free_view(f->ov);
     delete f;
     return 0;
@@ -418,6 +502,43 @@ int build_sell(const CsrView& a, int32_t sigma, SellC** out, cudaStream_t s) {
         k_sell_fill<T><<<blocks_for(n), 256, 0, s>>>(a.ptr, a.idx, (const T*)a.val, f->perm, f->slice_len,
                                                       f->slice_ptr, n, f->col, (T*)f->val);
         GBK_LAUNCHED();
+    }
+    // warp work items
+    if (ns > 0) {
+        int32_t *cnt = nullptr, *mflag = nullptr, *mpos = nullptr;
+        GBK_CUDA(cudaMalloc(&cnt, 4 * (ns + 1)));
+        GBK_CUDA(cudaMalloc(&mflag, 4 * (ns + 1)));
+        GBK_CUDA(cudaMalloc(&mpos, 4 * (ns + 1)));
+        GBK_CUDA(cudaMalloc(&f->slice_item0, 4 * (ns + 1)));
+        k_sell_item_counts<<<blocks_for(ns + 1), 256, 0, s>>>(f->slice_len, ns, cnt);
+        GBK_LAUNCHED();
+        int rc = cub_scan_excl(cnt, f->slice_item0, ns + 1, s);
+        if (rc) return rc;
+        int32_t ni = 0;
+        GBK_CUDA(cudaMemcpyAsync(&ni, f->slice_item0 + ns, 4, cudaMemcpyDeviceToHost, s));
+        GBK_CUDA(cudaStreamSynchronize(s));
+        f->nitems = ni;
+        GBK_CUDA(cudaMalloc(&f->item_slice, 4 * (ni > 0 ? ni : 1)));
+        GBK_CUDA(cudaMalloc(&f->item_j0, 4 * (ni > 0 ? ni : 1)));
+        GBK_CUDA(cudaMalloc(&f->item_out, sizeof(T) * kSellC * (ni > 0 ? ni : 1)));
+        GBK_CUDA(cudaMemsetAsync(mflag + ns, 0, 4, s));
+        k_sell_item_fill<<<blocks_for(ns), 256, 0, s>>>(cnt, f->slice_item0, ns, f->item_slice, f->item_j0, mflag);
+        GBK_LAUNCHED();
+        rc = cub_scan_excl(mflag, mpos, ns + 1, s);
+        if (rc) return rc;
+        int32_t nm = 0;
+        GBK_CUDA(cudaMemcpyAsync(&nm, mpos + ns, 4, cudaMemcpyDeviceToHost, s));
+        GBK_CUDA(cudaStreamSynchronize(s));
+        f->nmulti = nm;
+        GBK_CUDA(cudaMalloc(&f->multi, 4 * (nm > 0 ? nm : 1)));
+        if (nm > 0) {
+            k_compact_flags<<<blocks_for(ns), 256, 0, s>>>(mflag, mpos, ns, f->multi);
+            GBK_LAUNCHED();
+        }
+        GBK_CUDA(cudaStreamSynchronize(s));
+        cudaFree(cnt);
+        cudaFree(mflag);
+        cudaFree(mpos);
     }
     // overflow rows
     if (n > 0) {
@@ -649,10 +770,15 @@ int build_lav(const CsrView& a, int32_t seg_cols, float dense_frac, SegCsr** out
 
 template <int SR, typename T>
 int run_sell(const SellC* f, int accum, const T* x, T* y, cudaStream_t s) {
-    if (f->nslices > 0) {
-        k_sell_spmv<SR, T><<<blocks_for(f->nslices * 32), 256, 0, s>>>(f->slice_len, f->slice_ptr, f->col,
-                                                                       (const T*)f->val, f->perm, f->n, f->nslices,
-                                                                       x, y, accum);
+    if (f->nitems > 0) {
+        k_sell_items<SR, T><<<blocks_for(f->nitems * 32), 256, 0, s>>>(
+            f->item_slice, f->item_j0, f->slice_item0, f->slice_len, f->slice_ptr, f->col, (const T*)f->val, f->perm,
+            f->n, f->nitems, x, y, accum, (T*)f->item_out);
+        GBK_LAUNCHED();
+    }
+    if (f->nmulti > 0) {
+        k_sell_fold<SR, T><<<blocks_for(f->nmulti * kSellC), 256, 0, s>>>(
+            f->multi, f->nmulti, f->slice_item0, (const T*)f->item_out, f->perm, f->n, y, accum);
         GBK_LAUNCHED();
     }
     if (f->nov > 0) {
