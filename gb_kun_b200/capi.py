@@ -37,7 +37,7 @@ class GbkError(RuntimeError):
 
 class FormatParams(C.Structure):
     _fields_ = [("sell_c", C.c_int32), ("sell_sigma", C.c_int32), ("seg_cols", C.c_int32),
-                ("lav_dense_frac", C.c_float), ("csr_kernel", C.c_int32)]
+                ("lav_dense_frac", C.c_float), ("csr_kernel", C.c_int32), ("sell_hot_cols", C.c_int32)]
 
 
 class MatrixInfo(C.Structure):
@@ -48,19 +48,23 @@ class MatrixInfo(C.Structure):
 
 class TuneResult(C.Structure):
     _fields_ = [("format", C.c_int32), ("sell_sigma", C.c_int32), ("csr_kernel", C.c_int32), ("cached", C.c_int32),
-                ("ncandidates", C.c_int32), ("best_ms", C.c_float), ("candidate_ms", C.c_float * 8)]
+                ("ncandidates", C.c_int32), ("best_ms", C.c_float), ("candidate_ms", C.c_float * 12),
+                ("sell_hot_cols", C.c_int32)]
 
-    CANDIDATES = ["CSR_bins", "CSR_merge", "SELL_C_s1", "SELL_C_s256", "SELL_C_s4096", "CSR_SEG", "LAV"]
+    CANDIDATES = ["CSR_bins", "CSR_merge", "SELL_C_s1", "SELL_C_s256", "SELL_C_s4096", "CSR_SEG", "LAV",
+                  "SELL_C_s4096_hot16k", "SELL_C_s4096_hot52k", "SELL_C_s256_hot52k"]
 
     def describe(self) -> dict:
         names = {0: "CSR", 3: "CSR_SEG", 4: "LAV", 6: "SELL_C"}
         d = {"format": names.get(self.format, str(self.format)), "cached": bool(self.cached)}
         if self.format == 6:
             d["sigma"] = self.sell_sigma
+            d["hot_cols"] = self.sell_hot_cols
         if self.format == 0:
             d["csr_kernel"] = {1: "merge-path", 2: "degree-bins"}.get(self.csr_kernel, "default")
         if not self.cached:
-            d["candidate_ms"] = {n: round(self.candidate_ms[i], 4) for i, n in enumerate(self.CANDIDATES)}
+            d["candidate_ms"] = {n: round(self.candidate_ms[i], 4) for i, n in enumerate(self.CANDIDATES)
+                                 if i < self.ncandidates}
         return d
 
 
@@ -203,9 +207,11 @@ class Matrix:
         check(lib().gbk_matrix_get_info(self.h, C.byref(inf)), "gbk_matrix_get_info")
         return inf
 
-    def set_format(self, fmt: str, sell_c=0, sigma=0, seg_cols=0, lav_frac=0.0, csr_kernel=0, stream=None):
-        """Storage format; csr_kernel picks the CSR kernel (0 default bins, 1 merge-path, 2 bins)."""
-        p = FormatParams(sell_c, sigma, seg_cols, lav_frac, csr_kernel)
+    def set_format(self, fmt: str, sell_c=0, sigma=0, seg_cols=0, lav_frac=0.0, csr_kernel=0, hot_cols=0,
+                   stream=None):
+        """Storage format; csr_kernel picks the CSR kernel (0 default bins, 1 merge-path, 2 bins);
+        hot_cols > 0 stages the x values of the most used columns in shared memory (SELL-C)."""
+        p = FormatParams(sell_c, sigma, seg_cols, lav_frac, csr_kernel, hot_cols)
         check(lib().gbk_matrix_set_format(self.h, FMT[fmt], C.byref(p), stream_ptr(stream)), "gbk_matrix_set_format")
 
     def autotune(self, transpose=False, semiring="plus_times", reps=20, stream=None) -> TuneResult:

@@ -36,6 +36,8 @@ constexpr int kSellC = 32;
 constexpr int kSellMaxLen = 1 << 30;  // long slices are cut into work items instead
 constexpr int kSellChunk = 64;        // slice steps per work item (one warp)
 constexpr int kSellUnroll = 8;        // steps per pipelined load group
+constexpr int kHotThreads = 1024;     // persistent hot-x CTA: one per SM
+constexpr int kMaxHotBytes = 212992;  // shared memory for staged x (208 KiB)
 
 struct SellC {
     int64_t n = 0;           // rows
@@ -60,6 +62,11 @@ struct SellC {
     void* item_out = nullptr;        // 32 partials per item of a multi-item slice
     int64_t nmulti = 0;
     int32_t* multi = nullptr;        // slices with more than one item
+    // hot-x: columns renumbered by in-degree; x[0, hot) staged in shared memory
+    int32_t hot = 0;
+    int64_t ncols = 0;
+    int32_t* new_to_old = nullptr;
+    void* xr = nullptr;              // renumbered x (ncols)
 };
 
 struct SegCsr {
@@ -147,6 +154,89 @@ __global__ void __launch_bounds__(256) k_sell_items(const int32_t* __restrict__ 
     } else {
         item_out[k * kSellC + lane] = acc;
     }
+}
+
+// Hot-x variant: columns are renumbered by in-degree (descending), so the x
+// values of the `hot` most used columns form the prefix x[0, hot).  Each
+// persistent CTA copies that prefix into shared memory once, and gathers of
+// hot columns read shared memory instead of making an L2 round trip.
+template <int SR, typename T>
+__global__ void __launch_bounds__(kHotThreads) k_sell_items_hot(
+    const int32_t* __restrict__ item_slice, const int32_t* __restrict__ item_j0,
+    const int32_t* __restrict__ slice_item0, const int32_t* __restrict__ slice_len,
+    const int64_t* __restrict__ slice_ptr, const int32_t* __restrict__ col, const T* __restrict__ val,
+    const int32_t* __restrict__ perm, int64_t n, int64_t nitems, int hot, const T* __restrict__ x,
+    T* __restrict__ y, int accum, T* __restrict__ item_out) {
+    using S = Semiring<SR, T>;
+    constexpr int U = kSellUnroll;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sx = reinterpret_cast<T*>(smem_raw);
+    for (int i = threadIdx.x; i < hot; i += kHotThreads) sx[i] = x[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (kHotThreads / 32);
+    const uint64_t pol = policy_evict_last();
+    for (int64_t k = (int64_t)blockIdx.x * (kHotThreads / 32) + (threadIdx.x >> 5); k < nitems; k += warps) {
+        const int32_t s = item_slice[k];
+        const int32_t j0 = item_j0[k];
+        const int32_t j1 = min(j0 + kSellChunk, slice_len[s]);
+        const int64_t base = slice_ptr[s] + lane;
+        T acc = S::identity();
+        int c[U];
+        T a[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const bool in = j0 + u < j1;
+            c[u] = in ? ld_stream(col + base + (int64_t)(j0 + u) * kSellC) : -1;
+            a[u] = in ? ld_stream(val + base + (int64_t)(j0 + u) * kSellC) : T(0);
+        }
+        for (int j = j0; j < j1; j += U) {
+            int cn[U];
+            T an[U];
+            const int jn = j + U;
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const bool in = jn + u < j1;
+                cn[u] = in ? ld_stream(col + base + (int64_t)(jn + u) * kSellC) : -1;
+                an[u] = in ? ld_stream(val + base + (int64_t)(jn + u) * kSellC) : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (c[u] >= 0) {
+                    const T xv = c[u] < hot ? sx[c[u]] : ld_keep(x + c[u], pol);
+                    acc = S::add(acc, S::mul(a[u], xv));
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                c[u] = cn[u];
+                a[u] = an[u];
+            }
+        }
+        if (slice_item0[s + 1] - slice_item0[s] == 1) {
+            const int64_t p = (int64_t)s * kSellC + lane;
+            if (p < n) {
+                const int32_t r = perm[p];
+                y[r] = (accum == GBK_OP_SECOND) ? acc : binop<T>(accum, y[r], acc);
+            }
+        } else {
+            item_out[k * kSellC + lane] = acc;
+        }
+    }
+}
+
+// x in the renumbered column order: xr[i] = x[new_to_old[i]]
+template <typename T>
+__global__ void k_permute_x(const T* __restrict__ x, const int32_t* __restrict__ new_to_old, int64_t n,
+                            T* __restrict__ xr) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) xr[i] = x[new_to_old[i]];
+}
+
+// stored column ids -> renumbered ids (padding -1 stays)
+__global__ void k_renumber(int32_t* col, int64_t m, const int32_t* __restrict__ old_to_new) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e < m && col[e] >= 0) col[e] = old_to_new[col[e]];
 }
 
 // Slices cut into several items: fold the partials of each lane in item order.
@@ -414,6 +504,8 @@ int free_sell(SellC* f) {
     cudaFree(f->slice_item0);
     cudaFree(f->item_out);
     cudaFree(f->multi);
+    cudaFree(f->new_to_old);
+    cudaFree(f->xr);
     free_view(f->ov);
     delete f;
     return 0;
@@ -434,11 +526,78 @@ int free_seg(SegCsr* f) {
 // ---------------------------------------------------------------------------
 // SELL-C build
 
+__global__ void k_col_hist(const int32_t* __restrict__ idx, int64_t nnz, int32_t* __restrict__ cdeg) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e < nnz) atomicAdd(&cdeg[idx[e]], 1);
+}
+
+__global__ void k_hot_keys(const int32_t* cdeg, int64_t nc, uint32_t* key, int32_t* id) {
+    int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c < nc) {
+        key[c] = (uint32_t)(0x7fffffff - cdeg[c]);
+        id[c] = (int32_t)c;
+    }
+}
+
+__global__ void k_invert_perm(const int32_t* new_to_old, int64_t n, int32_t* old_to_new) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) old_to_new[new_to_old[i]] = (int32_t)i;
+}
+
+// Renumber columns by in-degree (descending, stable), as MatrixLAV does
+// (src/backend/matrix/containers/lav/build.hpp:113-141), and rewrite the
+// stored column ids, so the most used x values form the prefix x[0, hot).
+int renumber_hot(const CsrView& a, int32_t hot, SellC* f, cudaStream_t s) {
+    const int64_t nc = a.ncols;
+    int32_t *cdeg = nullptr, *id = nullptr, *old_to_new = nullptr;
+    uint32_t *key = nullptr, *key2 = nullptr;
+    GBK_CUDA(cudaMalloc(&cdeg, 4 * nc));
+    GBK_CUDA(cudaMalloc(&id, 4 * nc));
+    GBK_CUDA(cudaMalloc(&key, 4 * nc));
+    GBK_CUDA(cudaMalloc(&key2, 4 * nc));
+    GBK_CUDA(cudaMalloc(&old_to_new, 4 * nc));
+    GBK_CUDA(cudaMalloc(&f->new_to_old, 4 * nc));
+    GBK_CUDA(cudaMemsetAsync(cdeg, 0, 4 * nc, s));
+    if (a.nnz > 0) {
+        k_col_hist<<<blocks_for(a.nnz), 256, 0, s>>>(a.idx, a.nnz, cdeg);
+        GBK_LAUNCHED();
+    }
+    k_hot_keys<<<blocks_for(nc), 256, 0, s>>>(cdeg, nc, key, id);
+    GBK_LAUNCHED();
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, key, key2, id, f->new_to_old, (int)nc, 0, 32, s);
+    void* tmp = nullptr;
+    GBK_CUDA(cudaMalloc(&tmp, tb));
+    GBK_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, key, key2, id, f->new_to_old, (int)nc, 0, 32, s));
+    count_launch(1);
+    k_invert_perm<<<blocks_for(nc), 256, 0, s>>>(f->new_to_old, nc, old_to_new);
+    GBK_LAUNCHED();
+    if (f->padded > 0) {
+        k_renumber<<<blocks_for(f->padded), 256, 0, s>>>(f->col, f->padded, old_to_new);
+        GBK_LAUNCHED();
+    }
+    if (f->ov.nnz > 0) {
+        k_renumber<<<blocks_for(f->ov.nnz), 256, 0, s>>>(f->ov.idx, f->ov.nnz, old_to_new);
+        GBK_LAUNCHED();
+    }
+    GBK_CUDA(cudaMalloc(&f->xr, 4 * nc));  // 4-byte element types
+    f->hot = (int32_t)(hot < nc ? hot : nc);
+    GBK_CUDA(cudaStreamSynchronize(s));
+    cudaFree(tmp);
+    cudaFree(cdeg);
+    cudaFree(id);
+    cudaFree(key);
+    cudaFree(key2);
+    cudaFree(old_to_new);
+    return GBK_SUCCESS;
+}
+
 template <typename T>
-int build_sell(const CsrView& a, int32_t sigma, SellC** out, cudaStream_t s) {
+int build_sell(const CsrView& a, int32_t sigma, int32_t hot, SellC** out, cudaStream_t s) {
     SellC* f = new SellC();
     f->n = a.nrows;
     f->sigma = sigma;
+    f->ncols = a.ncols;
     const int64_t n = a.nrows;
     f->nslices = (n + kSellC - 1) / kSellC;
     int32_t* deg = nullptr;
@@ -587,6 +746,10 @@ int build_sell(const CsrView& a, int32_t sigma, SellC** out, cudaStream_t s) {
     cudaFree(is_ov);
     cudaFree(stored);
     cudaFree(deg);
+    if (hot > 0 && a.ncols > 0) {
+        int rc = renumber_hot(a, hot, f, s);
+        if (rc) return rc;
+    }
     *out = f;
     return GBK_SUCCESS;
 }
@@ -770,7 +933,24 @@ int build_lav(const CsrView& a, int32_t seg_cols, float dense_frac, SegCsr** out
 
 template <int SR, typename T>
 int run_sell(const SellC* f, int accum, const T* x, T* y, cudaStream_t s) {
-    if (f->nitems > 0) {
+    if (f->hot > 0) {
+        k_permute_x<T><<<blocks_for(f->ncols), 256, 0, s>>>(x, f->new_to_old, f->ncols, (T*)f->xr);
+        GBK_LAUNCHED();
+        x = (const T*)f->xr;
+        const int smem = (int)(f->hot * sizeof(T));
+        static bool attr_set = false;
+        if (!attr_set) {
+            GBK_CUDA(cudaFuncSetAttribute(k_sell_items_hot<SR, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          kMaxHotBytes));
+            attr_set = true;
+        }
+        if (f->nitems > 0) {
+            k_sell_items_hot<SR, T><<<(unsigned)num_sms(), kHotThreads, smem, s>>>(
+                f->item_slice, f->item_j0, f->slice_item0, f->slice_len, f->slice_ptr, f->col, (const T*)f->val,
+                f->perm, f->n, f->nitems, f->hot, x, y, accum, (T*)f->item_out);
+            GBK_LAUNCHED();
+        }
+    } else if (f->nitems > 0) {
         k_sell_items<SR, T><<<blocks_for(f->nitems * 32), 256, 0, s>>>(
             f->item_slice, f->item_j0, f->slice_item0, f->slice_len, f->slice_ptr, f->col, (const T*)f->val, f->perm,
             f->n, f->nitems, x, y, accum, (T*)f->item_out);
@@ -865,6 +1045,9 @@ int build_format(gbk_matrix A, gbk_format fmt, const gbk_format_params* p, cudaS
     if (prm.sell_sigma == 0) prm.sell_sigma = 4096;
     if (prm.seg_cols == 0) prm.seg_cols = 131072;
     if (prm.lav_dense_frac == 0.0f) prm.lav_dense_frac = 0.8f;
+    GBK_REQUIRE(prm.sell_hot_cols >= 0 && prm.sell_hot_cols * 4 <= kMaxHotBytes && prm.sell_hot_cols % 4 == 0,
+                GBK_INVALID_VALUE, "sell_hot_cols %d: a multiple of 4 up to %d", prm.sell_hot_cols,
+                kMaxHotBytes / 4);
     GBK_REQUIRE(prm.sell_c == kSellC, GBK_UNSUPPORTED, "SELL-C: slice height %d not provided (32 = one warp)",
                 prm.sell_c);
     GBK_REQUIRE(prm.sell_sigma >= 1 && prm.seg_cols >= 1 && prm.lav_dense_frac > 0.0f && prm.lav_dense_frac <= 1.0f,
@@ -883,8 +1066,8 @@ int build_format(gbk_matrix A, gbk_format fmt, const gbk_format_params* p, cudaS
     for (int o = 0; o < 2; o++) {
         const CsrView& v = o ? A->csc : A->csr;
         if (fmt == GBK_FMT_SELL_C) {
-            rc = A->vtype == GBK_F32 ? build_sell<float>(v, prm.sell_sigma, &A->sell[o], s)
-                                     : build_sell<int32_t>(v, prm.sell_sigma, &A->sell[o], s);
+            rc = A->vtype == GBK_F32 ? build_sell<float>(v, prm.sell_sigma, prm.sell_hot_cols, &A->sell[o], s)
+                                     : build_sell<int32_t>(v, prm.sell_sigma, prm.sell_hot_cols, &A->sell[o], s);
         } else if (fmt == GBK_FMT_CSR_SEG) {
             rc = A->vtype == GBK_F32 ? build_seg<float>(v, prm.seg_cols, &A->seg[o], s)
                                      : build_seg<int32_t>(v, prm.seg_cols, &A->seg[o], s);

@@ -23,12 +23,16 @@ struct Candidate {
     gbk_format fmt;
     int32_t sigma;
     int32_t kernel;
+    int32_t hot;
 };
 
+// Order matches gbk_tune_result.candidate_ms (include/gbk.h).
 const Candidate kCandidates[] = {
-    {GBK_FMT_CSR, 0, kKernelBins},      {GBK_FMT_CSR, 0, kKernelMerge},     {GBK_FMT_SELL_C, 1, kKernelAuto},
-    {GBK_FMT_SELL_C, 256, kKernelAuto}, {GBK_FMT_SELL_C, 4096, kKernelAuto}, {GBK_FMT_CSR_SEG, 0, kKernelAuto},
-    {GBK_FMT_LAV, 0, kKernelAuto},
+    {GBK_FMT_CSR, 0, kKernelBins, 0},        {GBK_FMT_CSR, 0, kKernelMerge, 0},
+    {GBK_FMT_SELL_C, 1, kKernelAuto, 0},     {GBK_FMT_SELL_C, 256, kKernelAuto, 0},
+    {GBK_FMT_SELL_C, 4096, kKernelAuto, 0},  {GBK_FMT_CSR_SEG, 0, kKernelAuto, 0},
+    {GBK_FMT_LAV, 0, kKernelAuto, 0},        {GBK_FMT_SELL_C, 4096, kKernelAuto, 16384},
+    {GBK_FMT_SELL_C, 4096, kKernelAuto, 53248}, {GBK_FMT_SELL_C, 256, kKernelAuto, 53248},
 };
 constexpr int kNumCandidates = sizeof(kCandidates) / sizeof(kCandidates[0]);
 
@@ -94,6 +98,7 @@ int apply_candidate(gbk_matrix A, const Candidate& c, cudaStream_t s) {
     gbk_format_params p = A->params;
     p.sell_sigma = c.sigma ? c.sigma : 4096;
     p.csr_kernel = c.kernel;
+    p.sell_hot_cols = c.hot;
     return build_format(A, c.fmt, &p, s);
 }
 
@@ -175,6 +180,7 @@ extern "C" int gbk_matrix_autotune(gbk_matrix A, int transpose, gbk_semiring sr,
     res.format = kCandidates[best].fmt;
     res.sell_sigma = kCandidates[best].sigma;
     res.csr_kernel = kCandidates[best].kernel;
+    res.sell_hot_cols = kCandidates[best].hot;
     res.best_ms = res.cached ? 0.0f : res.candidate_ms[best];
     if (result) *result = res;
     return GBK_SUCCESS;

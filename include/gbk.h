@@ -34,6 +34,9 @@ typedef struct gbk_format_params {
     int32_t seg_cols;        /* CSR_SEG / LAV column-segment width; default 131072 (512 KiB of f32 x) */
     float lav_dense_frac;    /* LAV: fraction of nnz in the dense column segments; default 0.8 */
     int32_t csr_kernel;      /* CSR kernel: 0 default (degree bins), 1 merge-path tiles, 2 degree bins */
+    int32_t sell_hot_cols;   /* SELL-C: columns renumbered by in-degree and the x values of the first
+                                sell_hot_cols (most used) columns staged in shared memory per CTA;
+                                0 = off; at most 53248 */
 } gbk_format_params;
 
 /* A mask argument: either dense (n entries of `dtype`, non-zero = set) or
@@ -93,7 +96,9 @@ typedef struct gbk_tune_result {
     int32_t cached;          /* 1 when the choice came from the cache (nothing was timed) */
     int32_t ncandidates;
     float best_ms;
-    float candidate_ms[8];   /* CSR bins, CSR merge-path, SELL-C sigma 1 / 256 / 4096, CSR_SEG, LAV */
+    float candidate_ms[12];  /* CSR bins, CSR merge-path, SELL-C sigma 1 / 256 / 4096, CSR_SEG, LAV,
+                                SELL-C sigma 4096 with 16384 / 53248 hot columns, sigma 256 with 53248 */
+    int32_t sell_hot_cols;   /* chosen hot-column count (SELL-C only) */
 } gbk_tune_result;
 
 /* Per-graph autotuner (no counterpart in the reference, which takes the

@@ -35,7 +35,16 @@ GRAPHS = {
     "hub": hub_graph,
 }
 
-FORMATS = [("SELL_C", 1), ("SELL_C", 256), ("SELL_C", 4096), ("CSR_SEG", 0), ("LAV", 0)]
+FORMATS = [("SELL_C", 1), ("SELL_C", 256), ("SELL_C", 4096), ("SELL_C_HOT", 4096), ("SELL_C_HOT", 1), ("CSR_SEG", 0),
+           ("LAV", 0)]
+
+
+def apply(A, fmt, sigma, seg_cols):
+    """SELL_C_HOT: SELL-C with 1024 shared-memory x columns."""
+    if fmt == "SELL_C_HOT":
+        A.set_format("SELL_C", sigma=sigma, hot_cols=1024)
+    else:
+        A.set_format(fmt, sigma=sigma, seg_cols=seg_cols if fmt != "SELL_C" else 0)
 
 
 def transposed(oracle, g, val):
@@ -52,7 +61,7 @@ def test_plus_times_f32(capi, oracle, gname, fmt, sigma, transpose):
     val = gg.values_f32(g, seed=1)
     x = gg.vector_f32(g.n, seed=2)
     A = capi.Matrix.from_graph(g, val)
-    A.set_format(fmt, sigma=sigma, seg_cols=1024 if fmt != "SELL_C" else 0)
+    apply(A, fmt, sigma, 1024)
     y = torch.full((g.n,), 5.0, device="cuda")
     A.mxv(dev(x), y, transpose=transpose, accum="plus")
     go, vo = transposed(oracle, g, val) if transpose else (g, val)
@@ -69,7 +78,7 @@ def test_exact_semirings_i32(capi, oracle, fmt, sigma, sr):
         x = (gg.vector_f32(g.n, seed=4) * 1000).astype(np.int32)
         x[::3] = 0
         A = capi.Matrix.from_graph(g, val)
-        A.set_format(fmt, sigma=sigma, seg_cols=512 if fmt != "SELL_C" else 0)
+        apply(A, fmt, sigma, 512)
         for transpose in (False, True):
             y0 = np.full(g.n, 9, np.int32)
             y = dev(y0)
