@@ -239,7 +239,8 @@ def format_sweep(args, peak):
     fmts = [("CSR_bins", {"fmt": "CSR", "csr_kernel": 2}), ("CSR_merge", {"fmt": "CSR", "csr_kernel": 1}),
             ("SELL_C_s1", {"fmt": "SELL_C", "sigma": 1}), ("SELL_C_s256", {"fmt": "SELL_C", "sigma": 256}),
             ("SELL_C_s4096", {"fmt": "SELL_C", "sigma": 4096}),
-            ("SELL_C_s4096_hot52k", {"fmt": "SELL_C", "sigma": 4096, "hot": 53248}),
+            ("SELL_C_s4096_reorder", {"fmt": "SELL_C", "sigma": 4096, "reorder": 1}),
+            ("SELL_C_s256_reorder", {"fmt": "SELL_C", "sigma": 256, "reorder": 1}),
             ("CSR_SEG", {"fmt": "CSR_SEG"}), ("LAV", {"fmt": "LAV"})]
     for gname in ("rmat", "er"):
         g = gg.rmat(args.scale, args.edge_factor, seed=args.seed) if gname == "rmat" else \
@@ -252,7 +253,8 @@ def format_sweep(args, peak):
         dx = torch.from_numpy(x).cuda()
         dy = torch.zeros(g.n, device="cuda")
         for name, f in fmts:
-            A.set_format(f["fmt"], sigma=f.get("sigma", 0), csr_kernel=f.get("csr_kernel", 0), hot_cols=f.get("hot", 0))
+            A.set_format(f["fmt"], sigma=f.get("sigma", 0), csr_kernel=f.get("csr_kernel", 0), hot_cols=f.get("hot", 0),
+                         reorder_cols=f.get("reorder", 0))
             ms = time_spmv(A, dx, dy, args.sweep_steps, 3)
             err = float(np.abs(dy.cpu().numpy().astype(np.float64) - ref).sum() / np.abs(ref).sum())
             ms_or = time_spmv(A, dx, dy, args.sweep_steps, 3, semiring="lor_land")

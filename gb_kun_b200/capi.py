@@ -37,7 +37,8 @@ class GbkError(RuntimeError):
 
 class FormatParams(C.Structure):
     _fields_ = [("sell_c", C.c_int32), ("sell_sigma", C.c_int32), ("seg_cols", C.c_int32),
-                ("lav_dense_frac", C.c_float), ("csr_kernel", C.c_int32), ("sell_hot_cols", C.c_int32)]
+                ("lav_dense_frac", C.c_float), ("csr_kernel", C.c_int32), ("sell_hot_cols", C.c_int32),
+                ("sell_reorder_cols", C.c_int32)]
 
 
 class MatrixInfo(C.Structure):
@@ -52,7 +53,8 @@ class TuneResult(C.Structure):
                 ("sell_hot_cols", C.c_int32)]
 
     CANDIDATES = ["CSR_bins", "CSR_merge", "SELL_C_s1", "SELL_C_s256", "SELL_C_s4096", "CSR_SEG", "LAV",
-                  "SELL_C_s4096_hot16k", "SELL_C_s4096_hot52k", "SELL_C_s256_hot52k"]
+                  "SELL_C_s4096_hot16k", "SELL_C_s4096_hot52k", "SELL_C_s256_hot52k", "SELL_C_s4096_reorder",
+                  "SELL_C_s256_reorder"]
 
     def describe(self) -> dict:
         names = {0: "CSR", 3: "CSR_SEG", 4: "LAV", 6: "SELL_C"}
@@ -208,10 +210,11 @@ class Matrix:
         return inf
 
     def set_format(self, fmt: str, sell_c=0, sigma=0, seg_cols=0, lav_frac=0.0, csr_kernel=0, hot_cols=0,
-                   stream=None):
+                   reorder_cols=0, stream=None):
         """Storage format; csr_kernel picks the CSR kernel (0 default bins, 1 merge-path, 2 bins);
-        hot_cols > 0 stages the x values of the most used columns in shared memory (SELL-C)."""
-        p = FormatParams(sell_c, sigma, seg_cols, lav_frac, csr_kernel, hot_cols)
+        hot_cols > 0 stages the x values of the most used columns in shared memory (SELL-C);
+        reorder_cols renumbers columns by in-degree (SELL-C)."""
+        p = FormatParams(sell_c, sigma, seg_cols, lav_frac, csr_kernel, hot_cols, reorder_cols)
         check(lib().gbk_matrix_set_format(self.h, FMT[fmt], C.byref(p), stream_ptr(stream)), "gbk_matrix_set_format")
 
     def autotune(self, transpose=False, semiring="plus_times", reps=20, stream=None) -> TuneResult:

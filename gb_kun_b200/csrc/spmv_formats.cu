@@ -593,7 +593,7 @@ int renumber_hot(const CsrView& a, int32_t hot, SellC* f, cudaStream_t s) {
 }
 
 template <typename T>
-int build_sell(const CsrView& a, int32_t sigma, int32_t hot, SellC** out, cudaStream_t s) {
+int build_sell(const CsrView& a, int32_t sigma, int32_t hot, int32_t reorder, SellC** out, cudaStream_t s) {
     SellC* f = new SellC();
     f->n = a.nrows;
     f->sigma = sigma;
@@ -746,7 +746,7 @@ int build_sell(const CsrView& a, int32_t sigma, int32_t hot, SellC** out, cudaSt
     cudaFree(is_ov);
     cudaFree(stored);
     cudaFree(deg);
-    if (hot > 0 && a.ncols > 0) {
+    if ((hot > 0 || reorder) && a.ncols > 0) {
         int rc = renumber_hot(a, hot, f, s);
         if (rc) return rc;
     }
@@ -933,10 +933,12 @@ int build_lav(const CsrView& a, int32_t seg_cols, float dense_frac, SegCsr** out
 
 template <int SR, typename T>
 int run_sell(const SellC* f, int accum, const T* x, T* y, cudaStream_t s) {
-    if (f->hot > 0) {
+    if (f->new_to_old) {  // renumbered columns: gather x into the new order first
         k_permute_x<T><<<blocks_for(f->ncols), 256, 0, s>>>(x, f->new_to_old, f->ncols, (T*)f->xr);
         GBK_LAUNCHED();
         x = (const T*)f->xr;
+    }
+    if (f->hot > 0) {
         const int smem = (int)(f->hot * sizeof(T));
         static bool attr_set = false;
         if (!attr_set) {
@@ -1066,8 +1068,10 @@ int build_format(gbk_matrix A, gbk_format fmt, const gbk_format_params* p, cudaS
     for (int o = 0; o < 2; o++) {
         const CsrView& v = o ? A->csc : A->csr;
         if (fmt == GBK_FMT_SELL_C) {
-            rc = A->vtype == GBK_F32 ? build_sell<float>(v, prm.sell_sigma, prm.sell_hot_cols, &A->sell[o], s)
-                                     : build_sell<int32_t>(v, prm.sell_sigma, prm.sell_hot_cols, &A->sell[o], s);
+            rc = A->vtype == GBK_F32
+                     ? build_sell<float>(v, prm.sell_sigma, prm.sell_hot_cols, prm.sell_reorder_cols, &A->sell[o], s)
+                     : build_sell<int32_t>(v, prm.sell_sigma, prm.sell_hot_cols, prm.sell_reorder_cols, &A->sell[o],
+                                           s);
         } else if (fmt == GBK_FMT_CSR_SEG) {
             rc = A->vtype == GBK_F32 ? build_seg<float>(v, prm.seg_cols, &A->seg[o], s)
                                      : build_seg<int32_t>(v, prm.seg_cols, &A->seg[o], s);

@@ -33,6 +33,7 @@ const Candidate kCandidates[] = {
     {GBK_FMT_SELL_C, 4096, kKernelAuto, 0},  {GBK_FMT_CSR_SEG, 0, kKernelAuto, 0},
     {GBK_FMT_LAV, 0, kKernelAuto, 0},        {GBK_FMT_SELL_C, 4096, kKernelAuto, 16384},
     {GBK_FMT_SELL_C, 4096, kKernelAuto, 53248}, {GBK_FMT_SELL_C, 256, kKernelAuto, 53248},
+    {GBK_FMT_SELL_C, 4096, kKernelAuto, -1},    {GBK_FMT_SELL_C, 256, kKernelAuto, -1},
 };
 constexpr int kNumCandidates = sizeof(kCandidates) / sizeof(kCandidates[0]);
 
@@ -98,7 +99,8 @@ int apply_candidate(gbk_matrix A, const Candidate& c, cudaStream_t s) {
     gbk_format_params p = A->params;
     p.sell_sigma = c.sigma ? c.sigma : 4096;
     p.csr_kernel = c.kernel;
-    p.sell_hot_cols = c.hot;
+    p.sell_hot_cols = c.hot > 0 ? c.hot : 0;
+    p.sell_reorder_cols = c.hot < 0 ? 1 : 0;  // hot == -1: renumbered columns, no staging
     return build_format(A, c.fmt, &p, s);
 }
 
@@ -180,7 +182,7 @@ extern "C" int gbk_matrix_autotune(gbk_matrix A, int transpose, gbk_semiring sr,
     res.format = kCandidates[best].fmt;
     res.sell_sigma = kCandidates[best].sigma;
     res.csr_kernel = kCandidates[best].kernel;
-    res.sell_hot_cols = kCandidates[best].hot;
+    res.sell_hot_cols = kCandidates[best].hot;  // -1: columns renumbered, x not staged
     res.best_ms = res.cached ? 0.0f : res.candidate_ms[best];
     if (result) *result = res;
     return GBK_SUCCESS;

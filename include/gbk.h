@@ -37,6 +37,8 @@ typedef struct gbk_format_params {
     int32_t sell_hot_cols;   /* SELL-C: columns renumbered by in-degree and the x values of the first
                                 sell_hot_cols (most used) columns staged in shared memory per CTA;
                                 0 = off; at most 53248 */
+    int32_t sell_reorder_cols; /* SELL-C: renumber columns by in-degree (most used first) so gathers of
+                                  popular x values share sectors and L1 lines; implied by sell_hot_cols */
 } gbk_format_params;
 
 /* A mask argument: either dense (n entries of `dtype`, non-zero = set) or
@@ -97,8 +99,9 @@ typedef struct gbk_tune_result {
     int32_t ncandidates;
     float best_ms;
     float candidate_ms[12];  /* CSR bins, CSR merge-path, SELL-C sigma 1 / 256 / 4096, CSR_SEG, LAV,
-                                SELL-C sigma 4096 with 16384 / 53248 hot columns, sigma 256 with 53248 */
-    int32_t sell_hot_cols;   /* chosen hot-column count (SELL-C only) */
+                                SELL-C sigma 4096 with 16384 / 53248 hot columns, sigma 256 with 53248,
+                                SELL-C sigma 4096 / 256 with renumbered columns */
+    int32_t sell_hot_cols;   /* chosen hot-column count (SELL-C only; -1 = renumbered columns only) */
 } gbk_tune_result;
 
 /* Per-graph autotuner (no counterpart in the reference, which takes the
