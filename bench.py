@@ -56,6 +56,7 @@ def parse():
     p.add_argument("--graph", default="rmat", choices=["rmat", "er"])
     p.add_argument("--format", default="auto", choices=["auto", "CSR", "SELL_C", "CSR_SEG", "LAV"],
                    help="storage format; auto = the per-graph autotuner's choice")
+    p.add_argument("--sigma", type=int, default=0, help="SELL-C sorting window for --format SELL_C")
     p.add_argument("--seed", type=int, default=42)
     p.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -197,17 +198,34 @@ def cpu_baseline(args, g, val, x):
                 "sample": f"failed: {e}"}
 
 
-def read_traffic(workload):
-    f = ROOT / "profiles" / f"{workload}.md"
+def read_traffic(profile):
+    """DRAM bytes of one SpMV from the committed ncu summary.
+
+    Prefers the whole-SpMV sum (`traffic_bytes_per_spmv:`, all kernels of one
+    SpMV from the launch list), else the dominant kernel's own launch."""
+    f = ROOT / "profiles" / f"{profile}.md"
     if not f.exists():
         return None
+    found = {}
     for line in f.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1].strip().split()[0])
-            except ValueError:
-                return None
-    return None
+        for key in ("traffic_bytes_per_spmv:", "traffic_bytes_per_launch:"):
+            if line.startswith(key) and key not in found:
+                try:
+                    found[key] = float(line.split(":", 1)[1].strip().split()[0])
+                except ValueError:
+                    pass
+    return found.get("traffic_bytes_per_spmv:", found.get("traffic_bytes_per_launch:"))
+
+
+def dominant_kernel(fmt_name, scale, graph):
+    """(kernel description, profile summary) for the storage format that ran."""
+    tag = f"{graph}{scale}"
+    if fmt_name == "SELL_C":
+        return ("k_sell_items (+ k_sell_fold; rows of problematic slices through k_spmv_binned); achieved counts "
+                "the whole SpMV", f"spmv_sell_c_{tag}")
+    if fmt_name == "CSR":
+        return "k_spmv_binned (+ k_spmv_split_fixup); achieved counts the whole SpMV", f"spmv_csr_kernels_{tag}"
+    return f"{fmt_name} kernels; achieved counts the whole SpMV", f"spmv_{fmt_name.lower()}_{tag}"
 
 
 def time_spmv(A, dx, dy, steps, warmup, semiring="plus_times"):
@@ -280,7 +298,7 @@ def run_ours(args):
     if args.format == "auto":
         tuned = A.autotune(reps=20).describe()
     else:
-        A.set_format(args.format)
+        A.set_format(args.format, sigma=args.sigma)
     stream = torch.cuda.current_stream()
     dx = torch.from_numpy(x).cuda()
     dy = torch.zeros(g.n, device="cuda")
@@ -341,6 +359,8 @@ def run_ours(args):
         ok = float(np.abs(got - ref).sum() / np.abs(ref).sum())
 
     peak, peak_kind = hbm_peak()
+    ran_format = tuned["format"] if tuned else args.format
+    kern_desc, kern_profile = dominant_kernel(ran_format, args.scale, args.graph)
     achieved = B / (avg_kernel_ms * 1e-3) / 1e9
     value = world * B / (ms_per_step * 1e-3) / 1e9
     cfg = workload_config(args, g)
@@ -358,8 +378,8 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                      if peak_kind == "measured" else "fallback 6650 GB/s",
-                     "traffic": read_traffic(cfg["workload"]),
-                     "kernel": "k_spmv_merge (+ k_spmv_fixup), timed together per step",
+                     "traffic": read_traffic(kern_profile),
+                     "kernel": kern_desc,
                      "algorithmic_bytes_per_launch": B},
         "e2e": {"value": round(world * B / (e2e_ms * 1e-3) / 1e9, 2), "unit": "GB/s",
                 "h2d_bytes_per_step": 4 * g.n, "d2h_bytes_per_step": 4 * g.n, "ms_per_step": round(e2e_ms, 5)},
