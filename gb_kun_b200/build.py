@@ -36,6 +36,7 @@ CU_SOURCES = [
     "vector_ops.cu",
     "spgemm.cu",
     "tune.cu",
+    "noalloc.cu",
     "batched.cu",
 ]
 

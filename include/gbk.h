@@ -170,6 +170,18 @@ int gbk_vec_nvals(const void* v, gbk_dtype t, int64_t n, int64_t* out, void* str
  * *nvals on the host; synchronises the stream. */
 int gbk_vec_to_sparse(const void* dense, gbk_dtype t, int64_t n, int32_t* ids, void* vals, int64_t* nvals,
                       void* stream);
+/* The same conversion without allocating device memory (no counterpart in
+ * the reference).  For callers that cannot allocate at call time: a host
+ * framework whose caching allocator already holds the free device memory,
+ * a serving loop that must not wait on the allocator mid-request, an
+ * application that budgets device memory up front.  Its scratch is a fixed
+ * ~32 KiB array inside the library, held on every GPU that loads it until
+ * exit, so n is limited to 33,554,432 (larger n: GBK_INVALID_VALUE).  All
+ * calls share the scratch: calls that overlap on the GPU race.  The first
+ * call on each device looks up the scratch address; make it before any
+ * stream capture begins.  Synchronises the stream. */
+int gbk_vec_to_sparse_noalloc(const void* dense, gbk_dtype t, int64_t n, int32_t* ids, void* vals,
+                              int64_t* nvals, void* stream);
 /* Sparse -> dense: zero fill, then scatter (DenseVector::convert, dense_vector.hpp:87-102). */
 int gbk_vec_to_dense(const int32_t* ids, const void* vals, int64_t nvals, gbk_dtype t, void* dense, int64_t n,
                      void* stream);
