@@ -108,6 +108,9 @@ def _declare(lib):
         "gbk_matrix_csr_arrays": ([vp, ci, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), vp], ci),
         "gbk_matrix_set_format": ([vp, ci, C.POINTER(FormatParams), vp], ci),
         "gbk_mxv": ([vp, ci, ci, ci, ci, vp, vp, vp, ci, ci, vp], ci),
+        "gbk_msbfs": ([vp, vp, ci, vp, ci, vp, vp], ci),
+        "gbk_ppr": ([vp, vp, ci, C.c_double, C.c_double, ci, vp, vp, vp], ci),
+        "gbk_sssp_multi": ([vp, vp, ci, vp, vp, vp], ci),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name, None)
@@ -252,6 +255,33 @@ class Matrix:
                                ptr(x_vals), int(x_ids.numel()), ptr(y), C.byref(mask) if mask is not None else None,
                                stream_ptr(stream)), "gbk_spmspv")
         return y
+
+    def msbfs(self, sources, levels, direction=0, stream=None):
+        """BFS levels from up to 64 sources at once into levels (device int32, len(sources) x n).
+        Returns each source's largest level."""
+        src = np.ascontiguousarray(sources, dtype=np.int32)
+        depths = np.zeros(len(src), dtype=np.int32)
+        check(lib().gbk_msbfs(self.h, ptr(src), len(src), ptr(levels), int(direction), ptr(depths),
+                              stream_ptr(stream)), "gbk_msbfs")
+        return depths
+
+    def ppr(self, seeds, ranks, damping=0.85, tol=1e-6, itermax=100, stream=None):
+        """Personalised PageRank for up to 32 seeds into ranks (device float32, len(seeds) x n).
+        Returns the iterations each seed ran."""
+        src = np.ascontiguousarray(seeds, dtype=np.int32)
+        iters = np.zeros(len(src), dtype=np.int32)
+        check(lib().gbk_ppr(self.h, ptr(src), len(src), float(damping), float(tol), int(itermax), ptr(ranks),
+                            ptr(iters), stream_ptr(stream)), "gbk_ppr")
+        return iters
+
+    def sssp_multi(self, sources, dist, stream=None):
+        """Integer-weight shortest paths from up to 32 sources into dist (device int32,
+        len(sources) x n; INT32_MAX = unreachable).  Returns the rounds each source ran."""
+        src = np.ascontiguousarray(sources, dtype=np.int32)
+        iters = np.zeros(len(src), dtype=np.int32)
+        check(lib().gbk_sssp_multi(self.h, ptr(src), len(src), ptr(dist), ptr(iters), stream_ptr(stream)),
+              "gbk_sssp_multi")
+        return iters
 
     def mxm_masked(self, A, B, semiring="plus_one", ctype=I32, stream=None):
         """C<self> = A (+.x) B with this matrix as the mask; returns a new Matrix."""

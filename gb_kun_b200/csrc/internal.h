@@ -38,6 +38,19 @@ struct CsrView {
 
 struct SellC;     // spmv_formats.cu
 struct SegCsr;    // spmv_formats.cu (CSR_SEG and LAV share one layout)
+struct Batch;     // batched.h
+
+// Tunables of the batched traversals (batched.cu).
+struct BatchOptions {
+    int bfs_direction = 0;    // 0 = auto, 1 = push only, 2 = pull only
+    int bfs_alpha = 4;        // switch to pull when frontier edges * alpha > unvisited edges
+    int bfs_beta = 24;        // switch back to push when frontier vertices * beta < n
+    int item_edges = 256;     // PPR / SSSP: edges per warp work item
+    float damping = 0.85f;    // PPR
+    double tol = 1e-6;        // PPR: stop when sum |r_new - r_old| < tol
+    int itermax = 100;        // PPR iteration cap
+    int sssp_max_iter = 0;    // SSSP iteration cap (0: n)
+};
 
 }  // namespace gbk
 
@@ -54,6 +67,9 @@ struct gbk_matrix_s {
     void* xcopy = nullptr;      // n elements, used when x aliases y
     int64_t xcopy_elems = 0;
     int device = 0;
+    // batches kept for the one-shot batched calls (BFS, PPR, SSSP)
+    gbk::Batch* batch[3] = {nullptr, nullptr, nullptr};
+    gbk::BatchOptions batch_opt[3];
 };
 
 namespace gbk {
@@ -64,6 +80,7 @@ int spmv_binned(const RowBins* rb, const CsrView& v, int sr, int accum, int dtyp
                 const void* mask, int mdt, int mmode, cudaStream_t s);
 
 int ensure_csc(gbk_matrix A, cudaStream_t s);
+void free_batches(gbk_matrix A);  // batched.cu
 int build_tiles(CsrView& v, int elem_bytes, cudaStream_t s);
 void free_view(CsrView& v);
 int free_formats(gbk_matrix A);

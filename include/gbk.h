@@ -160,6 +160,38 @@ int gbk_spmspv(gbk_matrix A, int transpose, gbk_semiring sr, gbk_binop accum, gb
 int gbk_mxm_masked(gbk_matrix* out, gbk_matrix M, gbk_matrix A, gbk_matrix B, gbk_semiring sr, gbk_dtype ctype,
                    void* stream);
 
+/* ---- batched traversals (many sources per launch) ----------------------- */
+
+/* Multi-source BFS: up to 64 sources advanced together, one bit of a uint64
+ * per vertex each.  Per source the result equals bfs_blast
+ * (algorithms/bfs/bfs.hpp:93-142, edges followed along the rows of A):
+ * levels[k * n + v] = depth of v from sources[k] (source 1, unreached 0).
+ * levels is device memory of nsources * n int32.  direction: 0 chooses push
+ * or pull per iteration, 1 push only, 2 pull only (same levels).  depths
+ * (host, may be NULL) receives each source's largest level.  The whole
+ * iteration loop runs as one CUDA graph; synchronises the stream.  The
+ * reference runs one source per call; the packing is this library's. */
+int gbk_msbfs(gbk_matrix A, const int32_t* sources, int nsources, int32_t* levels, int direction, int32_t* depths,
+              void* stream);
+/* Personalised PageRank for up to 32 seeds as one FP32 SpMM per iteration.
+ * Per seed it is the page_rank_sinks iteration (algorithms/pr/pr.hpp:20-153)
+ * with r0 = e_seed and the teleport and sink mass returned to the seed:
+ * r = [(1 - damping) + damping * sink] e_seed + A (r ./ d), d = max(coldeg,
+ * 1) / damping, stopping when sum |r_new - r| < tol (tol > 0) or after
+ * itermax iterations.  ranks is device memory of nseeds * n floats (row k =
+ * seed k); iters (host, may be NULL) receives the iterations per seed.
+ * Synchronises the stream. */
+int gbk_ppr(gbk_matrix A, const int32_t* seeds, int nseeds, double damping, double tol, int itermax, float* ranks,
+            int32_t* iters, void* stream);
+/* Single-source shortest paths from up to 32 sources with integer edge
+ * weights (the matrix values; GBK_F32 values are truncated to int32).
+ * dist[k * n + v] = shortest distance from sources[k] (INT32_MAX when
+ * unreachable), the fixpoint sssp_bellman_ford_blast reaches
+ * (algorithms/sssp/sssp_blast.hpp:8-72).  iters (host, may be NULL) receives
+ * the relaxation rounds per source.  Weights must be non-negative.
+ * Synchronises the stream. */
+int gbk_sssp_multi(gbk_matrix A, const int32_t* sources, int nsources, int32_t* dist, int32_t* iters, void* stream);
+
 /* ---- vectors ------------------------------------------------------------ */
 
 /* Count of non-zero entries (DenseVector::get_nvals, dense_vector.hpp:44-52).
