@@ -38,6 +38,7 @@ CU_SOURCES = [
     "tune.cu",
     "noalloc.cu",
     "batched.cu",
+    "serve.cu",
 ]
 
 LABLAS_SOURCES = ["lablas_capi.cpp"]

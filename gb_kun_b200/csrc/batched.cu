@@ -205,6 +205,58 @@ __global__ void k_extract_cols(const T* __restrict__ b0, const T* __restrict__ b
     }
 }
 
+// Per-lane result summaries; blockIdx.y is the lane.  KIND 0: BFS levels
+// in rows of `stride`; 1: PPR ranks [n][32] in b0 / b1 by which[lane];
+// 2: SSSP distances [n][32].
+template <int KIND>
+__global__ void k_digest(const void* __restrict__ b0, const void* __restrict__ b1, const int32_t* __restrict__ which,
+                         int64_t n, int64_t stride, unsigned long long mask, LaneDigest* out) {
+    const int lane = blockIdx.y;
+    if (!((mask >> lane) & 1)) return;
+    unsigned long long reached = 0, isum = 0;
+    double fsum = 0;
+    const float* fb = (KIND == 1 && (which[lane] & 1)) ? (const float*)b1 : (const float*)b0;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        if (KIND == 0) {
+            const int32_t x = ((const int32_t*)b0)[(int64_t)lane * stride + v];
+            if (x > 0) {
+                reached++;
+                isum += (unsigned long long)x;
+            }
+        } else if (KIND == 1) {
+            const float x = fb[v * 32 + lane];
+            if (x > 0.f) reached++;
+            fsum += (double)x;
+        } else {
+            const int32_t x = ((const int32_t*)b0)[v * 32 + lane];
+            if (x != INT_MAX) {
+                reached++;
+                isum += (unsigned long long)(long long)x;
+            }
+        }
+    }
+    reached = warp_sum64(reached);
+    isum = warp_sum64(isum);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) fsum += __shfl_xor_sync(kFull, fsum, o);
+    if ((threadIdx.x & 31) == 0) {
+        if (reached) atomicAdd((unsigned long long*)&out[lane].reached, reached);
+        if (isum) atomicAdd((unsigned long long*)&out[lane].isum, isum);
+        if (fsum != 0.0) atomicAdd(&out[lane].fsum, fsum);
+    }
+}
+
+template <int KIND>
+int launch_digest(const void* b0, const void* b1, const int32_t* which, int64_t n, int64_t stride,
+                  unsigned long long mask, int lanes, LaneDigest* out, cudaStream_t s) {
+    GBK_CUDA(cudaMemsetAsync(out, 0, sizeof(LaneDigest) * lanes, s));
+    if (!mask || n == 0) return GBK_SUCCESS;
+    const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 2));
+    k_digest<KIND><<<dim3(gx, lanes), 256, 0, s>>>(b0, b1, which, n, stride, mask, out);
+    GBK_LAUNCHED();
+    return GBK_SUCCESS;
+}
+
 struct Lanes64 {
     int32_t v[64];
 };
@@ -599,6 +651,11 @@ struct BfsBatch final : Batch {
                                      cfg.levels + (int64_t)(lane_lo + j) * cfg.stride, 4 * (size_t)cfg.n,
                                      cudaMemcpyDefault, s));
         return GBK_SUCCESS;
+    }
+
+    int digest(unsigned long long mask, LaneDigest* d_out, cudaStream_t s) override {
+        GBK_REQUIRE(!mask || cfg.levels, GBK_INVALID_OBJECT, "BFS digest: no lane has run yet");
+        return launch_digest<0>(cfg.levels, nullptr, nullptr, cfg.n, cfg.stride, mask, kBfsLanes, d_out, s);
     }
 
     int release(unsigned long long mask, cudaStream_t s) override {
@@ -1002,6 +1059,11 @@ struct PprBatch final : Batch {
         return GBK_SUCCESS;
     }
 
+    int digest(unsigned long long mask, LaneDigest* d_out, cudaStream_t s) override {
+        return launch_digest<1>(cfg.r[0], cfg.r[1], d_st->result_buf, cfg.n, 0, mask & 0xffffffffull, kColLanes,
+                                d_out, s);
+    }
+
     int release(unsigned long long mask, cudaStream_t s) override {
         k_cols_release<<<1, 1, 0, s>>>(&d_st->st, mask);
         GBK_LAUNCHED();
@@ -1238,6 +1300,10 @@ struct SsspBatch final : Batch {
             cfg.dist, cfg.dist, nullptr, cfg.n, lane_lo, nl, (int32_t*)dst, stride);
         GBK_LAUNCHED();
         return GBK_SUCCESS;
+    }
+
+    int digest(unsigned long long mask, LaneDigest* d_out, cudaStream_t s) override {
+        return launch_digest<2>(cfg.dist, nullptr, nullptr, cfg.n, 0, mask & 0xffffffffull, kColLanes, d_out, s);
     }
 
     int release(unsigned long long mask, cudaStream_t s) override {

@@ -39,6 +39,15 @@ struct BatchStatus {
 
 enum BatchKind { kBatchBfs = 0, kBatchPpr = 1, kBatchSssp = 2 };
 
+// Per-lane summary of a finished result: vertices reached (BFS level > 0,
+// finite distance, rank > 0), the integer sum (levels, distances) and the
+// float sum (ranks).
+struct LaneDigest {
+    long long reached;
+    long long isum;
+    double fsum;
+};
+
 struct Batch {
     virtual ~Batch() {}
     virtual int kind() const = 0;
@@ -56,6 +65,9 @@ struct Batch {
     // row j = lane lane_lo + j, row stride `stride` elements (levels int32,
     // ranks float, distances int32).
     virtual int extract(int lane_lo, int nl, void* dst, int64_t stride, cudaStream_t s) = 0;
+    // Summaries of the finished lanes in `mask` into d_out[lane] (device,
+    // lanes() entries; the masked entries are zeroed first).
+    virtual int digest(unsigned long long mask, LaneDigest* d_out, cudaStream_t s) = 0;
     // Make finished lanes idle again.
     virtual int release(unsigned long long mask, cudaStream_t s) = 0;
     // Device bytes held by the batch and the bytes of one lane's state.
