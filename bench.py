@@ -60,6 +60,15 @@ def parse():
     p.add_argument("--seed", type=int, default=42)
     p.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--mode", default="spmv", choices=["spmv", "batched", "serve", "algorithms"],
+                   help="spmv: the SpMV line (default); batched: 64-source BFS + 32-column PPR / SSSP on "
+                        "R-MAT s22; serve: Poisson request stream on a resident undirected R-MAT s24; "
+                        "algorithms: BFS/CC/PR/SSSP/TC on undirected R-MAT s23 vs the reference CPU code")
+    p.add_argument("--queries", type=int, default=1000, help="serve: requests in the trace")
+    p.add_argument("--rate", type=float, default=2000.0, help="serve: mean arrival rate (queries/s)")
+    p.add_argument("--serial-queries", type=int, default=60, help="serve: requests run one at a time")
+    p.add_argument("--serve-scale", type=int, default=24, help="serve: R-MAT scale of the resident graph")
+    p.add_argument("--alg-scale", type=int, default=23, help="algorithms: R-MAT scale")
     return p.parse_args()
 
 
@@ -399,6 +408,247 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def _median_ms(fn, reps):
+    """Median device time of fn() over reps calls (CUDA events on the current stream)."""
+    import torch
+    ts = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return statistics.median(ts), ts
+
+
+def _ref_threads():
+    try:
+        from oracle.cpu import Reference
+        return Reference() if Reference.available() else None
+    except Exception:
+        return None
+
+
+def run_batched(args):
+    """64-source BFS and 32-column PPR / SSSP on R-MAT scale 22 (directed)."""
+    import torch
+    from gb_kun_b200 import capi, graphgen as gg, lablas_capi as lc
+    capi.init(0)
+    g = gg.rmat(args.scale, args.edge_factor, seed=args.seed)
+    w = gg.weights_i32(g, seed=args.seed + 3)
+    A = capi.Matrix.from_graph(g, val=w.astype(np.float32))
+    deg = torch.from_numpy(np.diff(g.row_ptr).astype(np.int64)).cuda()
+    src = gg.sources(g, 64, seed=args.seed + 4)
+    reps = max(3, min(args.steps, 10))
+    warm = max(3, args.warmup)
+    lv = torch.zeros((64, g.n), dtype=torch.int32, device="cuda")
+    rk = torch.zeros((32, g.n), dtype=torch.float32, device="cuda")
+    dd = torch.zeros((32, g.n), dtype=torch.int32, device="cuda")
+    for _ in range(warm):
+        A.msbfs(src, lv)
+        A.ppr(src[:32], rk)
+        A.sssp_multi(src[:32], dd)
+    torch.cuda.synchronize()
+    l0 = capi.launch_count()
+    with ClockSampler(0) as clk:
+        bfs_ms, bfs_ts = _median_ms(lambda: A.msbfs(src, lv), reps)
+        ppr_ms, _ = _median_ms(lambda: A.ppr(src[:32], rk), reps)
+        sssp_ms, _ = _median_ms(lambda: A.sssp_multi(src[:32], dd), reps)
+    launches = capi.launch_count() - l0
+    depths = A.msbfs(src, lv)
+    ppr_it = A.ppr(src[:32], rk)
+    sssp_it = A.sssp_multi(src[:32], dd)
+    edges = int(((lv > 0).to(torch.int64) * deg).sum())
+    gteps = edges / (bfs_ms * 1e-3) / 1e9
+    # single-query paths, one at a time: lablas bfs_blast / sssp and one-lane PPR
+    G = lc.Graph(g, weights=w)
+    G.bfs(int(src[0]))
+    one_bfs = statistics.median([G.bfs(int(s))[1] for s in src[:8]])
+    G.sssp_i32(int(src[0]))
+    one_sssp = statistics.median([G.sssp_i32(int(s))[1] for s in src[:4]])
+    one_ppr, _ = _median_ms(lambda: A.ppr(src[:1], rk[:1]), 3)
+    # end to end: levels of all 64 sources back in pinned host memory
+    hl = torch.empty((64, g.n), dtype=torch.int32).pin_memory()
+    e2e_ms, _ = _median_ms(lambda: (A.msbfs(src, lv), hl.copy_(lv, non_blocking=True)), 3)
+    # checker: some lanes against the oracle
+    from oracle.cpu import Oracle
+    O = Oracle()
+    lvh, rkh, ddh = lv.cpu().numpy(), rk.cpu().numpy(), dd.cpu().numpy()
+    ok_bfs = all(np.array_equal(lvh[k], O.bfs(g, int(src[k]))) for k in (0, 31, 63))
+    d0 = O.sssp(g, w, int(src[0]))
+    ok_sssp = bool(np.array_equal(ddh[0], np.where(d0 < 0, np.iinfo(np.int32).max, d0).astype(np.int32)))
+    r0, _ = O.ppr(g, int(src[0]), tol=1e-6, itermax=100)
+    ppr_err = float(np.abs(rkh[0] - r0).sum() / np.abs(r0).sum())
+    # roofline of the PPR SpMM (per iteration, 32 columns): 4(n+1) + 4 nnz + 2 n 32 4
+    peak, peak_kind = hbm_peak()
+    spmm_bytes = 4 * (g.n + 1) + 4 * g.nnz + 2 * g.n * 32 * 4
+    spmm_gbs = spmm_bytes * int(ppr_it.max()) / (ppr_ms * 1e-3) / 1e9
+    R = _ref_threads()
+    cpu = None
+    if R is not None and not args.no_cpu_baseline:
+        r_edges, r_ms = 0, 0.0
+        for s in src[:2]:
+            lvr, ms = R.bfs(g, int(s))
+            r_edges += int(np.diff(g.row_ptr)[lvr > 0].sum())
+            r_ms += ms
+        cpu = {"value": round(r_edges / (r_ms * 1e-3) / 1e9, 4), "unit": "GTEPS", "cores": R.max_threads(),
+               "kind": "reference", "sample": "bfs_blast from 2 of the 64 sources, one at a time"}
+    out = {
+        "metric": "batched BFS GTEPS (64 sources per launch); PPR / SSSP queries/s",
+        "value": round(gteps, 3), "unit": "GTEPS", "n_gpus": 1, "steps": reps, "warmup": warm,
+        "ms_per_step": round(bfs_ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64 lanes (BFS), f32 (PPR), i32 (SSSP)", "data": "synthetic (seeded R-MAT, generated in-process)",
+        "config": {"workload": f"msbfs64_ppr32_sssp32_rmat{args.scale}", "n": g.n, "nnz": g.nnz,
+                   "graph": f"R-MAT scale {args.scale}, edge factor {args.edge_factor}, directed, seed {args.seed}",
+                   "sources": "64 seeded non-isolated vertices", "loop": "one CUDA graph per batch (while node)",
+                   "l2": "state and matrix larger than L2"},
+        "msbfs": {"ms": round(bfs_ms, 3), "edges_traversed": edges, "max_depth": int(depths.max()),
+                  "bfs_per_s": round(64 / (bfs_ms * 1e-3), 1), "one_at_a_time_ms": round(one_bfs, 3),
+                  "speedup_vs_one_at_a_time": round(64 * one_bfs / bfs_ms, 2), "bit_exact_checked": ok_bfs},
+        "ppr": {"ms": round(ppr_ms, 3), "seeds": 32, "iterations_max": int(ppr_it.max()),
+                "queries_per_s": round(32 / (ppr_ms * 1e-3), 1), "one_lane_ms": round(one_ppr, 3),
+                "rel_l1_vs_fp64_lane0": ppr_err},
+        "sssp": {"ms": round(sssp_ms, 3), "sources": 32, "rounds_max": int(sssp_it.max()),
+                 "queries_per_s": round(32 / (sssp_ms * 1e-3), 1), "one_at_a_time_ms": round(one_sssp, 3),
+                 "speedup_vs_one_at_a_time": round(32 * one_sssp / sssp_ms, 2), "bit_exact_checked": ok_sssp},
+        "roofline": {"bound": "hbm", "kernel": "k_ppr_spmm (+ k_ppr_fix, k_ppr_control); bytes per iteration "
+                                               "4(n+1) + 4 nnz + 2*n*32*4",
+                     "achieved": round(spmm_gbs, 2), "peak": peak, "unit": "GB/s", "frac": round(spmm_gbs / peak, 4),
+                     "traffic": None},
+        "e2e": {"value": round(edges / (e2e_ms * 1e-3) / 1e9, 3), "unit": "GTEPS", "h2d_bytes_per_step": 4 * 64,
+                "d2h_bytes_per_step": 4 * 64 * g.n, "ms_per_step": round(e2e_ms, 3)},
+        "gpu_launches": int(launches), "clocks": clk.summary(), "cpu_baseline": cpu,
+    }
+    print(json.dumps(out), flush=True)
+
+
+def run_serve(args):
+    """Poisson stream of BFS / SSSP / PPR requests on a resident undirected R-MAT graph."""
+    import torch
+    from gb_kun_b200 import capi, graphgen as gg, lablas_capi as lc
+    from gb_kun_b200.serve import Server, latency_stats, poisson_trace
+    capi.init(0)
+    t_gen = time.time()
+    g = gg.rmat(args.serve_scale, args.edge_factor, seed=args.seed, undirected=True)
+    w = gg.weights_i32(g, seed=args.seed + 3)
+    t_gen = time.time() - t_gen
+    A = capi.Matrix.from_graph(g, val=w.astype(np.float32))
+    cand = gg.sources(g, 1 << 16, seed=args.seed + 5)
+    arr, kinds, srcs = poisson_trace(args.queries, args.rate, mix=(0.5, 0.25, 0.25), candidates=cand,
+                                     seed=args.seed + 6)
+    nq = len(arr)
+    srv = Server(A, iters_per_launch=4)
+    # warm-up: builds the three batches and their graphs
+    wa, wk, ws = poisson_trace(12, 1e5, candidates=cand, seed=args.seed + 7)
+    srv.run_trace(wa, wk, ws)
+    l0 = capi.launch_count()
+    with ClockSampler(0) as clk:
+        res, wall = srv.run_trace(arr, kinds, srcs)
+    launches = capi.launch_count() - l0
+    burst, wall_b = srv.run_trace(np.zeros(nq), kinds, srcs)
+    used, budget, nb = srv.memory()
+    srv.close()
+    # one query at a time through the same engine (one lane, nothing overlaps)
+    m = min(args.serial_queries, nq)
+    one = Server(A, lanes_per_batch=1, max_inflight=1)
+    one.run_trace(wa[:3], wk[:3], ws[:3])
+    res1, wall1 = one.run_trace(arr[:m], kinds[:m], srcs[:m])
+    one_b, wall1_b = one.run_trace(np.zeros(m), kinds[:m], srcs[:m])
+    one.close()
+    # plain single-query algorithms (lablas bfs_blast / sssp), per-query device time
+    G = lc.Graph(g, weights=w)
+    G.bfs(int(cand[0]))
+    plain_bfs = statistics.median([G.bfs(int(s))[1] for s in cand[1:6]])
+    plain_sssp = statistics.median([G.sssp_i32(int(s))[1] for s in cand[1:4]])
+    G.close()
+    ser = {k: float(np.mean((one_b["t_done"] - one_b["t_admit"])[one_b["kind"] == k]) * 1e3)
+           if (one_b["kind"] == k).any() else None for k in (0, 1, 2)}
+    # one-at-a-time capacity with the faster single-query path per kind
+    best = {0: min(x for x in (ser[0], plain_bfs) if x), 1: ser[1], 2: min(x for x in (ser[2], plain_sssp) if x)}
+    mix = {0: 0.5, 1: 0.25, 2: 0.25}
+    one_best_qps = 1e3 / sum(mix[k] * best[k] for k in mix if best[k])
+    qps = nq / wall
+    cap = nq / wall_b
+    cap1 = m / wall1_b
+    lat = latency_stats(res)
+    out = {
+        "metric": "served-query QPS + p50/p99 vs one-at-a-time GPU", "value": round(qps, 2), "unit": "queries/s",
+        "n_gpus": 1, "steps": nq, "warmup": 12, "ms_per_step": round(1e3 * wall / nq, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64 lanes (BFS), f32 (PPR), i32 (SSSP)",
+        "data": "synthetic (seeded R-MAT, seeded Poisson trace)",
+        "config": {"workload": f"serve_rmat{args.serve_scale}u_poisson{int(args.rate)}",
+                   "graph": f"R-MAT scale {args.serve_scale}, edge factor {args.edge_factor}, undirected, "
+                            f"int32 weights in [1,255] as FP32 values", "n": g.n, "nnz": g.nnz,
+                   "trace": f"{nq} queries, Poisson mean {args.rate}/s, 50% BFS / 25% SSSP / 25% PPR, sources "
+                            "uniform over non-isolated vertices", "iters_per_launch": 4,
+                   "l2": "graph and batch state larger than L2"},
+        "latency_ms": lat, "qps_offered": args.rate, "qps_capacity_burst": round(cap, 2),
+        "batches": nb, "device_bytes_used": used, "memory_budget": budget,
+        "one_at_a_time": {"qps_poisson": round(m / wall1, 2), "qps_capacity": round(cap1, 2),
+                          "latency_ms": latency_stats(res1), "queries": m,
+                          "service_ms_engine": ser, "service_ms_plain_lablas": {"bfs": plain_bfs, "sssp": plain_sssp},
+                          "qps_capacity_best_single_query_path": round(one_best_qps, 2)},
+        "speedup_qps_vs_one_at_a_time": round(cap / max(cap1, one_best_qps), 2),
+        "e2e": {"value": round(qps, 2), "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 24, "note": "requests enter and summaries leave through the host loop"},
+        "gpu_launches": int(launches), "clocks": clk.summary(), "graph_gen_s": round(t_gen, 1),
+    }
+    print(json.dumps(out), flush=True)
+
+
+def run_algorithms(args):
+    """BFS, CC, PageRank, SSSP and TC on undirected R-MAT (lablas:: path) vs the reference CPU code."""
+    from gb_kun_b200 import capi, graphgen as gg, lablas_capi as lc
+    capi.init(0)
+    g = gg.rmat(args.alg_scale, args.edge_factor, seed=args.seed, undirected=True)
+    w = gg.weights_i32(g, seed=args.seed + 3)
+    G = lc.Graph(g, weights=w)
+    src = gg.sources(g, 4, seed=args.seed + 4)
+    R = _ref_threads()
+    degs = np.diff(g.row_ptr)
+    res = {}
+
+    def rec(name, gpu_ms, ref_ms, exact, extra=None):
+        res[name] = {"gpu_ms": round(gpu_ms, 3), "ref_cpu_ms": None if ref_ms is None else round(ref_ms, 1),
+                     "speedup": None if not ref_ms else round(ref_ms / gpu_ms, 1), "matches_reference": exact}
+        if extra:
+            res[name].update(extra)
+
+    G.bfs(int(src[0]))
+    lv, ms = G.bfs(int(src[1]))
+    ref = R.bfs(g, int(src[1])) if R else (None, None)
+    teps = int(degs[lv > 0].sum()) / (ms * 1e-3) / 1e9
+    rec("bfs", ms, ref[1], None if ref[0] is None else bool(np.array_equal(lv, ref[0])), {"gteps": round(teps, 3)})
+    lab, ms = G.cc()
+    lab, ms = G.cc()
+    ref = R.cc(g) if R else (None, None)
+    rec("cc", ms, ref[1], None if ref[0] is None else bool(np.array_equal(lab, ref[0])))
+    d, ms = G.sssp_f32(int(src[2]))
+    ref = R.sssp(g, w, int(src[2])) if R else (None, None)
+    rec("sssp", ms, ref[1], None if ref[0] is None else bool(np.array_equal(d, ref[0])))
+    r, it, ms = G.pagerank(itermax=100, damping=0.85, tol=1e-6)
+    ref = R.pagerank(g, it) if R else (None, None)
+    err = None if ref[0] is None else float(np.abs(r - ref[0]).sum() / np.abs(ref[0]).sum())
+    rec("pagerank", ms, ref[1], None if err is None else err < 1e-5, {"iterations": it, "rel_l1_vs_reference": err})
+    t, ms = G.tc()
+    rec("tc", ms, None, None, {"triangles": t})
+    out = {
+        "metric": "full algorithms: device time per run vs the reference CPU code", "value": res["bfs"]["gteps"],
+        "unit": "GTEPS (BFS)", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": res["bfs"]["gpu_ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 / i32",
+        "data": "synthetic (seeded R-MAT, generated in-process)",
+        "config": {"workload": f"algorithms_rmat{args.alg_scale}u", "n": g.n, "nnz": g.nnz,
+                   "graph": f"R-MAT scale {args.alg_scale}, edge factor {args.edge_factor}, undirected",
+                   "timing": "host timer around each lablas:: algorithm call (device work synchronised)"},
+        "algorithms": res,
+        "cpu_baseline": None if R is None else {"value": None, "unit": "ms", "cores": R.max_threads(),
+                                                "kind": "reference", "sample": "one run per algorithm"},
+    }
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -431,7 +681,9 @@ def run_reference(args):
 
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.mode != "spmv":
+        {"batched": run_batched, "serve": run_serve, "algorithms": run_algorithms}[args.mode](args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

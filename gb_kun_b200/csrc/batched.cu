@@ -89,14 +89,18 @@ int build_loop(LoopGraph& g, Body&& body) {
 
 struct RowItems {
     int64_t nitems = 0, nsplit = 0, nslots = 0;
-    int32_t* item_row = nullptr;
-    int32_t* item_beg = nullptr;
-    int32_t* item_slot = nullptr;    // -1: the piece is the whole row
+    int32_t* item_row = nullptr;     // first row
+    int32_t* item_end = nullptr;     // one past the last row
+    int32_t* item_beg = nullptr;     // first edge
+    int32_t* item_ee = nullptr;      // one past the last edge
+    int32_t* item_slot = nullptr;    // >= 0: piece of a split row, its partial-sum slot
     int32_t* split_row = nullptr;    // nsplit
     int32_t* split_first = nullptr;  // nsplit + 1 slot offsets
     void release() {
         cudaFree(item_row);
+        cudaFree(item_end);
         cudaFree(item_beg);
+        cudaFree(item_ee);
         cudaFree(item_slot);
         cudaFree(split_row);
         cudaFree(split_first);
@@ -104,15 +108,27 @@ struct RowItems {
     }
 };
 
-__global__ void k_item_counts(const int32_t* __restrict__ rp, int64_t n, int C, int32_t* cnt, int32_t* scnt,
-                              int32_t* sflag) {
+// Rows of more than C entries are cut into pieces of C.  Without grouping
+// every other row is one item; with grouping, consecutive short rows share
+// an item until the edge offset crosses a multiple of C or 32 rows are taken
+// (so an item holds at most 2C edges and 32 rows).
+__device__ __forceinline__ bool group_start(const int32_t* __restrict__ rp, int64_t v, int C) {
+    if (v == 0 || (v & 31) == 0) return true;
+    const int32_t prev = rp[v] - rp[v - 1];
+    return prev > C || rp[v] / C != rp[v - 1] / C;
+}
+
+__global__ void k_item_counts(const int32_t* __restrict__ rp, int64_t n, int C, int grouped, int32_t* cnt,
+                              int32_t* scnt, int32_t* sflag) {
     const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (v < n) {
         const int32_t deg = rp[v + 1] - rp[v];
-        const int32_t c = deg <= C ? 1 : (deg + C - 1) / C;
+        const bool big = deg > C;
+        int32_t c = big ? (deg + C - 1) / C : 1;
+        if (!big && grouped && !group_start(rp, v, C)) c = 0;
         cnt[v] = c;
-        scnt[v] = c > 1 ? c : 0;
-        sflag[v] = c > 1;
+        scnt[v] = big ? c : 0;
+        sflag[v] = big;
     } else if (v == n) {
         cnt[n] = 0;
         scnt[n] = 0;
@@ -122,7 +138,8 @@ __global__ void k_item_counts(const int32_t* __restrict__ rp, int64_t n, int C, 
 
 __global__ void k_item_fill(const int32_t* __restrict__ rp, int64_t n, int C, const int32_t* __restrict__ off,
                             const int32_t* __restrict__ soff, const int32_t* __restrict__ sidx, int32_t* item_row,
-                            int32_t* item_beg, int32_t* item_slot, int32_t* split_row, int32_t* split_first) {
+                            int32_t* item_end, int32_t* item_beg, int32_t* item_ee, int32_t* item_slot,
+                            int32_t* split_row, int32_t* split_first) {
     const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (v > n) return;
     if (v == n) {
@@ -130,29 +147,40 @@ __global__ void k_item_fill(const int32_t* __restrict__ rp, int64_t n, int C, co
         return;
     }
     const int32_t c = off[v + 1] - off[v];
-    const int32_t b = rp[v];
-    for (int32_t j = 0; j < c; ++j) {
-        item_row[off[v] + j] = (int32_t)v;
-        item_beg[off[v] + j] = b + j * C;
-        item_slot[off[v] + j] = c > 1 ? soff[v] + j : -1;
-    }
-    if (c > 1) {
+    if (c == 0) return;  // inside a group that an earlier row starts
+    const int32_t b = rp[v], e = rp[v + 1];
+    if (e - b > C) {
+        for (int32_t j = 0; j < c; ++j) {
+            const int32_t i = off[v] + j;
+            item_row[i] = (int32_t)v;
+            item_end[i] = (int32_t)v + 1;
+            item_beg[i] = b + j * C;
+            item_ee[i] = min(b + (j + 1) * C, e);
+            item_slot[i] = soff[v] + j;
+        }
         split_row[sidx[v]] = (int32_t)v;
         split_first[sidx[v]] = soff[v];
+        return;
     }
+    // the item runs to the next row that starts one (at most 32 rows on)
+    int64_t r = v + 1;
+    while (r < n && off[r + 1] == off[r]) ++r;
+    const int32_t i = off[v];
+    item_row[i] = (int32_t)v;
+    item_end[i] = (int32_t)r;
+    item_beg[i] = b;
+    item_ee[i] = rp[r];
+    item_slot[i] = -1;
 }
 
-int build_items(const CsrView& a, int C, RowItems& it, cudaStream_t s) {
+int build_items(const CsrView& a, int C, bool grouped, RowItems& it, cudaStream_t s) {
     const int64_t n = a.nrows;
     int32_t *cnt = nullptr, *off = nullptr;
     GBK_CUDA(cudaMallocAsync(&cnt, sizeof(int32_t) * 3 * (n + 1), s));
     GBK_CUDA(cudaMallocAsync(&off, sizeof(int32_t) * 3 * (n + 1), s));
-    int32_t *scnt = cnt + (n + 1), *sflag = cnt + 2 * (n + 1);
     int32_t *soff = off + (n + 1), *sidx = off + 2 * (n + 1);
-    (void)scnt;
-    (void)sflag;
     const unsigned g = (unsigned)((n + 1 + 255) / 256);
-    k_item_counts<<<g, 256, 0, s>>>(a.ptr, n, C, cnt, cnt + (n + 1), cnt + 2 * (n + 1));
+    k_item_counts<<<g, 256, 0, s>>>(a.ptr, n, C, grouped ? 1 : 0, cnt, cnt + (n + 1), cnt + 2 * (n + 1));
     GBK_LAUNCHED();
     size_t tb = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, off, (int)(n + 1), s);
@@ -170,13 +198,16 @@ int build_items(const CsrView& a, int C, RowItems& it, cudaStream_t s) {
     it.nitems = tot[0];
     it.nslots = tot[1];
     it.nsplit = tot[2];
-    GBK_CUDA(cudaMalloc(&it.item_row, sizeof(int32_t) * std::max<int64_t>(it.nitems, 1)));
-    GBK_CUDA(cudaMalloc(&it.item_beg, sizeof(int32_t) * std::max<int64_t>(it.nitems, 1)));
-    GBK_CUDA(cudaMalloc(&it.item_slot, sizeof(int32_t) * std::max<int64_t>(it.nitems, 1)));
+    const size_t ni = sizeof(int32_t) * std::max<int64_t>(it.nitems, 1);
+    GBK_CUDA(cudaMalloc(&it.item_row, ni));
+    GBK_CUDA(cudaMalloc(&it.item_end, ni));
+    GBK_CUDA(cudaMalloc(&it.item_beg, ni));
+    GBK_CUDA(cudaMalloc(&it.item_ee, ni));
+    GBK_CUDA(cudaMalloc(&it.item_slot, ni));
     GBK_CUDA(cudaMalloc(&it.split_row, sizeof(int32_t) * std::max<int64_t>(it.nsplit, 1)));
     GBK_CUDA(cudaMalloc(&it.split_first, sizeof(int32_t) * (it.nsplit + 1)));
-    k_item_fill<<<g, 256, 0, s>>>(a.ptr, n, C, off, soff, sidx, it.item_row, it.item_beg, it.item_slot,
-                                  it.split_row, it.split_first);
+    k_item_fill<<<g, 256, 0, s>>>(a.ptr, n, C, off, soff, sidx, it.item_row, it.item_end, it.item_beg, it.item_ee,
+                                  it.item_slot, it.split_row, it.split_first);
     GBK_LAUNCHED();
     cudaFreeAsync(tmp, s);
     cudaFreeAsync(cnt, s);
@@ -677,7 +708,9 @@ struct ColCfg {
     int item_edges;
     int64_t n, nnz;
     const int32_t* item_row;
+    const int32_t* item_end;
     const int32_t* item_beg;
+    const int32_t* item_ee;
     const int32_t* item_slot;
     int64_t nitems;
     const int32_t* split_row;
@@ -690,7 +723,7 @@ struct ColCfg {
     float* w[2];
     float* split_acc;
     double* partial;  // [parts][2][32]
-    int32_t parts_main, parts_fix;
+    int32_t parts_main;  // blocks of k_ppr_update, one partial each
     // SSSP
     int32_t* dist;
     uint32_t* chg[2];
@@ -709,18 +742,10 @@ struct PprState {
     double damping, tol;
 };
 
-__device__ __forceinline__ void ppr_epilogue(const ColCfg* __restrict__ cfg, int64_t row, float acc, bool mine,
-                                             int32_t seed, float tele, const float* __restrict__ r_old, float* r_out,
-                                             float* w_out, double& sink, double& rd) {
-    const int lane = threadIdx.x & 31;
-    const float rn = (row == seed) ? tele + acc : acc;
-    if (mine) {
-        const int64_t o = row * 32 + lane;
-        r_out[o] = rn;
-        w_out[o] = rn / cfg->d[row];
-        rd += (double)fabsf(r_old[o] - rn);
-        if (cfg->cdeg[row] == 0) sink += (double)rn;
-    }
+// The SpMM leaves each non-empty row's sum for the active lanes in r_out;
+// k_ppr_update turns it into the new rank.
+__device__ __forceinline__ void ppr_store_sum(float* r_out, int64_t row, float acc, bool mine) {
+    if (mine) __stcs(r_out + row * 32 + (threadIdx.x & 31), acc);
 }
 
 // Per-block sums of the warps' lane partials, in warp order (deterministic).
@@ -741,95 +766,136 @@ __device__ __forceinline__ void block_partials(double sink, double rd, double* o
     }
 }
 
-// One warp per work item, lane k = column k: the warp loads 32 column ids
-// at a time and gathers the 128-byte w rows of those vertices; pieces of
-// split rows park their sums for k_ppr_fix.
+// One warp per work item, lane k = column k.  An item is either a run of up
+// to 32 consecutive short rows or one piece of a long row; the warp loads 32
+// column ids at a time and keeps 8 gathers of 128-byte w rows in flight
+// whatever the row lengths, closing each row when the edge index passes its
+// end (rows are summed in CSR order, as the reference's loop does).  Lanes of
+// inactive columns issue no loads.  Pieces of split rows park their sums for
+// k_ppr_fix.
 __global__ void __launch_bounds__(kBT) k_ppr_spmm(const ColCfg* __restrict__ cfg, const PprState* __restrict__ st) {
     const unsigned act = (unsigned)st->st.active;
     const int lane = threadIdx.x & 31;
     const int cur = st->st.iter & 1;
     const float* __restrict__ w_in = cfg->w[cur];
-    const float* __restrict__ r_old = cfg->r[cur];
     float* r_out = cfg->r[cur ^ 1];
-    float* w_out = cfg->w[cur ^ 1];
     const bool mine = (act >> lane) & 1;
-    const int32_t seed = st->seed[lane];
-    const float tele = st->tele[lane];
     const int32_t* __restrict__ rp = cfg->rp;
     const int32_t* __restrict__ col = cfg->col;
-    const int C = cfg->item_edges;
-    double sink = 0, rd = 0;
+    const uint64_t pol = policy_evict_last();
     if (act) {
         const int64_t nitems = cfg->nitems;
         const int64_t gw = ((int64_t)blockIdx.x * kBT + threadIdx.x) >> 5;
         const int64_t nw = ((int64_t)gridDim.x * kBT) >> 5;
         for (int64_t it = gw; it < nitems; it += nw) {
-            const int32_t row = cfg->item_row[it];
-            const int32_t beg = cfg->item_beg[it];
-            const int32_t end = min(beg + C, rp[row + 1]);
+            int32_t row = cfg->item_row[it];
+            const int32_t row_end = cfg->item_end[it];
+            const int32_t eb = cfg->item_beg[it], ee = cfg->item_ee[it];
+            const int32_t slot = cfg->item_slot[it];
+            int32_t bound = slot >= 0 ? ee : rp[row + 1];
             float acc = 0.f;
-            for (int32_t e0 = beg; e0 < end; e0 += 32) {
-                const int cnt = min(32, end - e0);
+            for (int32_t e0 = eb; e0 < ee; e0 += 32) {
+                const int cnt = min(32, ee - e0);
                 const int32_t cl = lane < cnt ? __ldcs(col + e0 + lane) : 0;
-                int j = 0;
-                for (; j + 8 <= cnt; j += 8) {
+                for (int j = 0; j < cnt; j += 8) {
                     float t[8];
 #pragma unroll
                     for (int q = 0; q < 8; ++q) {
-                        const int32_t u = __shfl_sync(kFull, cl, j + q);
-                        t[q] = __ldg(w_in + (int64_t)u * 32 + lane);
+                        const int32_t u = __shfl_sync(kFull, cl, (j + q) & 31);
+                        t[q] = (mine && j + q < cnt) ? ld_keep(w_in + (int64_t)u * 32 + lane, pol) : 0.f;
                     }
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) acc += t[q];
-                }
-                for (; j < cnt; ++j) {
-                    const int32_t u = __shfl_sync(kFull, cl, j);
-                    acc += __ldg(w_in + (int64_t)u * 32 + lane);
+                    for (int q = 0; q < 8; ++q) {
+                        if (j + q < cnt) {
+                            const int32_t e = e0 + j + q;
+                            while (e >= bound) {  // rows that end here (empty rows need no store)
+                                if (bound > rp[row]) ppr_store_sum(r_out, row, acc, mine);
+                                acc = 0.f;
+                                ++row;
+                                bound = rp[row + 1];
+                            }
+                            acc += t[q];
+                        }
+                    }
                 }
             }
-            const int32_t slot = cfg->item_slot[it];
             if (slot >= 0) {
                 cfg->split_acc[(int64_t)slot * 32 + lane] = acc;
                 continue;
             }
-            ppr_epilogue(cfg, row, acc, mine, seed, tele, r_old, r_out, w_out, sink, rd);
+            if (row < row_end && rp[row + 1] > rp[row]) ppr_store_sum(r_out, row, acc, mine);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBT) k_ppr_fix(const ColCfg* __restrict__ cfg, const PprState* __restrict__ st) {
+    const unsigned act = (unsigned)st->st.active;
+    if (!act) return;
+    const int lane = threadIdx.x & 31;
+    float* r_out = cfg->r[(st->st.iter & 1) ^ 1];
+    const bool mine = (act >> lane) & 1;
+    const int64_t gw = ((int64_t)blockIdx.x * kBT + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * kBT) >> 5;
+    for (int64_t i = gw; i < cfg->nsplit; i += nw) {
+        float acc = 0.f;
+        for (int32_t sl = cfg->split_first[i]; sl < cfg->split_first[i + 1]; ++sl)
+            acc += cfg->split_acc[(int64_t)sl * 32 + lane];
+        ppr_store_sum(r_out, cfg->split_row[i], acc, mine);
+    }
+}
+
+// Elementwise step over all n x 32 entries (coalesced, thread t always on
+// column t % 32): rank = row sum (0 for empty rows) plus the teleport at the
+// seed, w = rank / d, and the per-column partial sums of |rank - old| and of
+// the rank held by sinks, per block in a fixed order.
+__global__ void __launch_bounds__(kBT) k_ppr_update(const ColCfg* __restrict__ cfg, const PprState* __restrict__ st) {
+    const unsigned act = (unsigned)st->st.active;
+    const int lane = threadIdx.x & 31;
+    const bool mine = (act >> lane) & 1;
+    double sink = 0, rd = 0;
+    if (mine) {
+        const int cur = st->st.iter & 1;
+        const float* __restrict__ r_old = cfg->r[cur];
+        float* r_out = cfg->r[cur ^ 1];
+        float* w_out = cfg->w[cur ^ 1];
+        const int32_t seed = st->seed[lane];
+        const float tele = st->tele[lane];
+        const int32_t* __restrict__ rp = cfg->rp;
+        const int64_t total = cfg->n * 32;
+        for (int64_t i = (int64_t)blockIdx.x * kBT + threadIdx.x; i < total; i += (int64_t)gridDim.x * kBT) {
+            const int64_t v = i >> 5;
+            const float acc = rp[v + 1] > rp[v] ? __ldcs(r_out + i) : 0.f;
+            const float rn = (v == seed) ? tele + acc : acc;
+            __stcs(r_out + i, rn);
+            __stcs(w_out + i, rn / cfg->d[v]);
+            rd += (double)fabsf(__ldcs(r_old + i) - rn);
+            if (cfg->cdeg[v] == 0) sink += (double)rn;
         }
     }
     block_partials(sink, rd, cfg->partial + (int64_t)blockIdx.x * 64);
 }
 
-__global__ void __launch_bounds__(kBT) k_ppr_fix(const ColCfg* __restrict__ cfg, const PprState* __restrict__ st) {
-    const unsigned act = (unsigned)st->st.active;
-    const int lane = threadIdx.x & 31;
-    const int cur = st->st.iter & 1;
-    const float* __restrict__ r_old = cfg->r[cur];
-    float* r_out = cfg->r[cur ^ 1];
-    float* w_out = cfg->w[cur ^ 1];
-    const bool mine = (act >> lane) & 1;
-    const int32_t seed = st->seed[lane];
-    const float tele = st->tele[lane];
+// 1024 threads: thread (g, k) sums the parts g, g + 32, ... of column k, then
+// warp 0 adds the 32 group sums in order (a fixed order: deterministic).
+__global__ void __launch_bounds__(1024) k_ppr_control(const ColCfg* __restrict__ cfg, PprState* st,
+                                                      cudaGraphConditionalHandle h) {
+    __shared__ double s_sink[32][33], s_rd[32][33];
+    const int k = threadIdx.x & 31, grp = threadIdx.x >> 5;
+    const int parts = cfg->parts_main;
     double sink = 0, rd = 0;
-    if (act) {
-        const int64_t gw = ((int64_t)blockIdx.x * kBT + threadIdx.x) >> 5;
-        const int64_t nw = ((int64_t)gridDim.x * kBT) >> 5;
-        for (int64_t i = gw; i < cfg->nsplit; i += nw) {
-            const int32_t row = cfg->split_row[i];
-            float acc = 0.f;
-            for (int32_t sl = cfg->split_first[i]; sl < cfg->split_first[i + 1]; ++sl)
-                acc += cfg->split_acc[(int64_t)sl * 32 + lane];
-            ppr_epilogue(cfg, row, acc, mine, seed, tele, r_old, r_out, w_out, sink, rd);
-        }
-    }
-    block_partials(sink, rd, cfg->partial + (int64_t)(cfg->parts_main + blockIdx.x) * 64);
-}
-
-__global__ void k_ppr_control(const ColCfg* __restrict__ cfg, PprState* st, cudaGraphConditionalHandle h) {
-    const int k = threadIdx.x;  // 32 threads
-    const int parts = cfg->parts_main + cfg->parts_fix;
-    double sink = 0, rd = 0;
-    for (int p = 0; p < parts; ++p) {
+    for (int p = grp; p < parts; p += 32) {
         sink += cfg->partial[(int64_t)p * 64 + k];
         rd += cfg->partial[(int64_t)p * 64 + 32 + k];
+    }
+    s_sink[grp][k] = sink;
+    s_rd[grp][k] = rd;
+    __syncthreads();
+    if (grp != 0) return;
+    sink = 0;
+    rd = 0;
+    for (int g2 = 0; g2 < 32; ++g2) {
+        sink += s_sink[g2][k];
+        rd += s_rd[g2][k];
     }
     const unsigned act = (unsigned)st->st.active;
     const int cur = st->st.iter & 1;
@@ -856,20 +922,20 @@ __global__ void k_ppr_control(const ColCfg* __restrict__ cfg, PprState* st, cuda
     }
 }
 
-// New columns start from r = e_seed, w = r / d.
-__global__ void k_ppr_init_cols(const ColCfg* __restrict__ cfg, const PprState* __restrict__ st, unsigned mask,
-                                Lanes32 seeds) {
+// New columns start from r = e_seed, w = r / d.  Only the new lanes are
+// touched: thread i covers row i / nl and lane lanes[i % nl].
+__global__ void k_ppr_init_cols(const ColCfg* __restrict__ cfg, const PprState* __restrict__ st, Lanes32 lanes,
+                                int nl, Lanes32 seeds) {
     const int cur = st->st.iter & 1;
     float* r = cfg->r[cur];
     float* w = cfg->w[cur];
-    const int64_t total = cfg->n * 32;
+    const int64_t total = cfg->n * nl;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int k = (int)(i & 31);
-        if (!((mask >> k) & 1)) continue;
-        const int64_t v = i >> 5;
+        const int64_t v = i / nl;
+        const int k = lanes.v[i - v * nl];
         const float x = (v == seeds.v[k]) ? 1.0f : 0.0f;
-        r[i] = x;
-        w[i] = x / cfg->d[v];
+        r[v * 32 + k] = x;
+        w[v * 32 + k] = x / cfg->d[v];
     }
 }
 
@@ -909,12 +975,13 @@ __global__ void k_ppr_degree(const int32_t* __restrict__ cp, int64_t n, float da
 }
 
 // shared set-up of the column-lane batches
-int init_col_cfg(gbk_matrix A, const BatchOptions& o, ColCfg& cfg, RowItems& items, cudaStream_t s) {
+int init_col_cfg(gbk_matrix A, const BatchOptions& o, bool grouped, ColCfg& cfg, RowItems& items,
+                 cudaStream_t s) {
     const CsrView& a = A->csr;
     GBK_REQUIRE(a.nrows == a.ncols, GBK_DIMENSION_MISMATCH, "batched traversal: matrix must be square");
     GBK_REQUIRE(o.item_edges >= 32 && o.item_edges % 32 == 0 && o.item_edges <= (1 << 20), GBK_INVALID_VALUE,
                 "batched traversal: item_edges must be a multiple of 32 in [32, 2^20]");
-    int rc = build_items(a, o.item_edges, items, s);
+    int rc = build_items(a, o.item_edges, grouped, items, s);
     if (rc) return rc;
     cfg.rp = a.ptr;
     cfg.col = a.idx;
@@ -924,7 +991,9 @@ int init_col_cfg(gbk_matrix A, const BatchOptions& o, ColCfg& cfg, RowItems& ite
     cfg.n = a.nrows;
     cfg.nnz = a.nnz;
     cfg.item_row = items.item_row;
+    cfg.item_end = items.item_end;
     cfg.item_beg = items.item_beg;
+    cfg.item_ee = items.item_ee;
     cfg.item_slot = items.item_slot;
     cfg.nitems = items.nitems;
     cfg.split_row = items.split_row;
@@ -942,7 +1011,7 @@ struct PprBatch final : Batch {
     PprState* d_st = nullptr;
     BatchStatus* h_st = nullptr;
     LoopGraph loop;
-    int grid_main = 0, grid_fix = 0;
+    int grid_main = 0, grid_fix = 0, grid_upd = 0;
     size_t bytes = 0;
 
     ~PprBatch() override {
@@ -962,12 +1031,12 @@ struct PprBatch final : Batch {
     const BatchStatus* host() const override { return h_st; }
     size_t device_bytes() const override { return bytes; }
     size_t lane_bytes() const override { return (size_t)cfg.n * 16; }
-    int kernels_per_iter() const override { return 3; }
+    int kernels_per_iter() const override { return 4; }
 
     int init(gbk_matrix a, const BatchOptions& o, cudaStream_t s) {
         A = a;
         opt = o;
-        int rc = init_col_cfg(A, o, cfg, items, s);
+        int rc = init_col_cfg(A, o, true, cfg, items, s);
         if (rc) return rc;
         rc = ensure_csc(A, s);  // column degrees
         if (rc) return rc;
@@ -992,9 +1061,9 @@ struct PprBatch final : Batch {
         GBK_CUDA(cudaMalloc(&cfg.split_acc, 4 * 32 * (size_t)std::max<int64_t>(items.nslots, 1)));
         grid_main = persistent_blocks((const void*)k_ppr_spmm, kBT);
         grid_fix = (int)std::max<int64_t>(1, std::min<int64_t>(grid_main, (items.nsplit * 32 + kBT - 1) / kBT));
-        cfg.parts_main = grid_main;
-        cfg.parts_fix = grid_fix;
-        GBK_CUDA(cudaMalloc(&cfg.partial, sizeof(double) * 64 * (grid_main + grid_fix)));
+        grid_upd = persistent_blocks((const void*)k_ppr_update, kBT);
+        cfg.parts_main = grid_upd;
+        GBK_CUDA(cudaMalloc(&cfg.partial, sizeof(double) * 64 * grid_upd));
         GBK_CUDA(cudaMalloc(&d_cfg, sizeof(ColCfg)));
         GBK_CUDA(cudaMalloc(&d_st, sizeof(PprState)));
         GBK_CUDA(cudaMallocHost(&h_st, sizeof(BatchStatus)));
@@ -1008,13 +1077,15 @@ struct PprBatch final : Batch {
         for (int k = 0; k < 32; ++k) init.result_buf[k] = -1;
         GBK_CUDA(cudaMemcpyAsync(d_st, &init, sizeof(PprState), cudaMemcpyHostToDevice, s));
         GBK_CUDA(cudaStreamSynchronize(s));
-        bytes = 8 * nn + 4 * 4 * 32 * nn + 4 * 32 * (size_t)items.nslots + 12 * (size_t)items.nitems;
+        bytes = 8 * nn + 4 * 4 * 32 * nn + 4 * 32 * (size_t)items.nslots + 20 * (size_t)items.nitems;
         return build_loop(loop, [&](cudaStream_t cs, cudaGraphConditionalHandle h) -> int {
             k_ppr_spmm<<<grid_main, kBT, 0, cs>>>(d_cfg, d_st);
             GBK_LAUNCH_CHECK();
             k_ppr_fix<<<grid_fix, kBT, 0, cs>>>(d_cfg, d_st);
             GBK_LAUNCH_CHECK();
-            k_ppr_control<<<1, 32, 0, cs>>>(d_cfg, d_st, h);
+            k_ppr_update<<<grid_upd, kBT, 0, cs>>>(d_cfg, d_st);
+            GBK_LAUNCH_CHECK();
+            k_ppr_control<<<1, 1024, 0, cs>>>(d_cfg, d_st, h);
             GBK_LAUNCH_CHECK();
             return GBK_SUCCESS;
         });
@@ -1030,10 +1101,14 @@ struct PprBatch final : Batch {
                             "batched PPR: seed %d out of range [0, %lld)", src[k], (long long)cfg.n);
                 l.v[k] = src[k];
             }
-        const int64_t total = cfg.n * 32;
+        Lanes32 nlist{};
+        int nl = 0;
+        for (int k = 0; k < kColLanes; ++k)
+            if ((mask >> k) & 1) nlist.v[nl++] = k;
+        const int64_t total = cfg.n * nl;
         const unsigned g = (unsigned)std::min<int64_t>((total + 255) / 256, (int64_t)num_sms() * 16);
         if (g > 0) {
-            k_ppr_init_cols<<<g, 256, 0, s>>>(d_cfg, d_st, (unsigned)mask, l);
+            k_ppr_init_cols<<<g, 256, 0, s>>>(d_cfg, d_st, nlist, nl, l);
             GBK_LAUNCHED();
         }
         k_ppr_admit<<<1, 32, 0, s>>>(d_cfg, d_st, (unsigned)mask, l, (double)opt.damping, opt.tol, opt.itermax);
@@ -1173,12 +1248,12 @@ __global__ void k_sssp_control(SsspState* st, cudaGraphConditionalHandle h) {
     }
 }
 
-__global__ void k_sssp_init_cols(const ColCfg* __restrict__ cfg, unsigned mask, Lanes32 src) {
-    const int64_t total = cfg->n * 32;
+__global__ void k_sssp_init_cols(const ColCfg* __restrict__ cfg, Lanes32 lanes, int nl, Lanes32 src) {
+    const int64_t total = cfg->n * nl;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int k = (int)(i & 31);
-        if (!((mask >> k) & 1)) continue;
-        cfg->dist[i] = ((i >> 5) == src.v[k]) ? 0 : INT_MAX;
+        const int64_t v = i / nl;
+        const int k = lanes.v[i - v * nl];
+        cfg->dist[v * 32 + k] = (v == src.v[k]) ? 0 : INT_MAX;
     }
 }
 
@@ -1232,7 +1307,7 @@ struct SsspBatch final : Batch {
     int init(gbk_matrix a, const BatchOptions& o, cudaStream_t s) {
         A = a;
         opt = o;
-        int rc = init_col_cfg(A, o, cfg, items, s);
+        int rc = init_col_cfg(A, o, false, cfg, items, s);
         if (rc) return rc;
         const size_t nn = (size_t)std::max<int64_t>(cfg.n, 1);
         GBK_CUDA(cudaMalloc(&cfg.dist, 4 * 32 * nn));
@@ -1251,7 +1326,7 @@ struct SsspBatch final : Batch {
         init.max_iter = max_iter();
         GBK_CUDA(cudaMemcpyAsync(d_st, &init, sizeof(SsspState), cudaMemcpyHostToDevice, s));
         GBK_CUDA(cudaStreamSynchronize(s));
-        bytes = 4 * 32 * nn + 8 * nn + 12 * (size_t)items.nitems;
+        bytes = 4 * 32 * nn + 8 * nn + 20 * (size_t)items.nitems;
         return build_loop(loop, [&](cudaStream_t cs, cudaGraphConditionalHandle h) -> int {
             k_sssp_push<<<grid_main, kBT, 0, cs>>>(d_cfg, d_st);
             GBK_LAUNCH_CHECK();
@@ -1273,10 +1348,14 @@ struct SsspBatch final : Batch {
                             "batched SSSP: source %d out of range [0, %lld)", src[k], (long long)cfg.n);
                 l.v[k] = src[k];
             }
-        const int64_t total = cfg.n * 32;
+        Lanes32 nlist{};
+        int nl = 0;
+        for (int k = 0; k < kColLanes; ++k)
+            if ((mask >> k) & 1) nlist.v[nl++] = k;
+        const int64_t total = cfg.n * nl;
         const unsigned g = (unsigned)std::min<int64_t>((total + 255) / 256, (int64_t)num_sms() * 16);
         if (g > 0) {
-            k_sssp_init_cols<<<g, 256, 0, s>>>(d_cfg, (unsigned)mask, l);
+            k_sssp_init_cols<<<g, 256, 0, s>>>(d_cfg, nlist, nl, l);
             GBK_LAUNCHED();
         }
         k_sssp_admit<<<1, 32, 0, s>>>(d_cfg, d_st, (unsigned)mask, l, max_iter());
