@@ -1450,6 +1450,10 @@ int bfs_batch_set_levels(Batch* b, int32_t* levels, int64_t stride, cudaStream_t
     return static_cast<BfsBatch*>(b)->set_levels(levels, stride, s);
 }
 
+BatchOptions base_options(gbk_matrix A, int kind) {
+    return A->batch_tuned[kind] ? A->batch_tuned_opt[kind] : BatchOptions{};
+}
+
 void free_batches(gbk_matrix A) {
     for (auto& p : A->batch) {
         delete p;
@@ -1498,12 +1502,12 @@ int gbk_msbfs(gbk_matrix A, const int32_t* sources, int nsources, int32_t* level
         GBK_REQUIRE(sources[i] >= 0 && sources[i] < A->csr.nrows, GBK_INVALID_INDEX,
                     "gbk_msbfs: source %d out of range", sources[i]);
     cudaStream_t s = (cudaStream_t)stream;
-    BatchOptions o;
+    const BatchOptions o = base_options(A, kBatchBfs);
     Batch* b = nullptr;
     int rc = cached_batch(A, kBatchBfs, o, &b, s);
     if (rc) return rc;
     BfsBatch* bb = static_cast<BfsBatch*>(b);
-    rc = bb->set_mode(direction, o.bfs_alpha, o.bfs_beta, s);
+    rc = bb->set_mode(direction == 0 ? o.bfs_direction : direction, o.bfs_alpha, o.bfs_beta, s);
     if (rc) return rc;
     rc = bb->set_levels(levels, A->csr.nrows, s);
     if (rc) return rc;
@@ -1523,7 +1527,7 @@ int gbk_ppr(gbk_matrix A, const int32_t* seeds, int nseeds, double damping, doub
         GBK_REQUIRE(seeds[i] >= 0 && seeds[i] < A->csr.nrows, GBK_INVALID_INDEX, "gbk_ppr: seed %d out of range",
                     seeds[i]);
     cudaStream_t s = (cudaStream_t)stream;
-    BatchOptions o;
+    BatchOptions o = base_options(A, kBatchPpr);
     o.damping = (float)damping;
     o.tol = tol;
     o.itermax = itermax;
@@ -1542,7 +1546,7 @@ int gbk_sssp_multi(gbk_matrix A, const int32_t* sources, int nsources, int32_t* 
         GBK_REQUIRE(sources[i] >= 0 && sources[i] < A->csr.nrows, GBK_INVALID_INDEX,
                     "gbk_sssp_multi: source %d out of range", sources[i]);
     cudaStream_t s = (cudaStream_t)stream;
-    BatchOptions o;
+    const BatchOptions o = base_options(A, kBatchSssp);
     Batch* b = nullptr;
     int rc = cached_batch(A, kBatchSssp, o, &b, s);
     if (rc) return rc;
@@ -1550,3 +1554,99 @@ int gbk_sssp_multi(gbk_matrix A, const int32_t* sources, int nsources, int32_t* 
 }
 
 }  // extern "C"
+
+namespace {
+
+// Device time of one one-shot run (events on s around a synchronising call).
+int time_one_shot(Batch* b, int k, const int32_t* src, void* out, int64_t stride, bool extract, cudaStream_t s,
+                  float* ms) {
+    cudaEvent_t e0, e1;
+    GBK_CUDA(cudaEventCreate(&e0));
+    GBK_CUDA(cudaEventCreate(&e1));
+    int rc = run_one_shot(b, k, src, out, stride, nullptr, extract, s);  // warm-up
+    float best = 1e30f;
+    for (int r = 0; r < 2 && !rc; ++r) {
+        cudaEventRecord(e0, s);
+        rc = run_one_shot(b, k, src, out, stride, nullptr, extract, s);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float t = 0;
+        cudaEventElapsedTime(&t, e0, e1);
+        best = std::min(best, t);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = best;
+    return rc;
+}
+
+}  // namespace
+
+extern "C" int gbk_batch_autotune(gbk_matrix A, int kind, const int32_t* sources, int nsources,
+                                  gbk_batch_tune_result* out, void* stream) {
+    GBK_REQUIRE(A && sources && out, GBK_NULL_POINTER, "gbk_batch_autotune: NULL argument");
+    GBK_REQUIRE(kind >= 0 && kind <= 2, GBK_INVALID_VALUE, "gbk_batch_autotune: kind must be 0, 1 or 2");
+    const int lanes = kind == kBatchBfs ? kBfsLanes : kColLanes;
+    GBK_REQUIRE(nsources >= 1 && nsources <= lanes, GBK_INVALID_VALUE, "gbk_batch_autotune: 1 to %d sources", lanes);
+    const int64_t n = A->csr.nrows;
+    for (int i = 0; i < nsources; ++i)
+        GBK_REQUIRE(sources[i] >= 0 && sources[i] < n, GBK_INVALID_INDEX, "gbk_batch_autotune: source out of range");
+    cudaStream_t s = (cudaStream_t)stream;
+    memset(out, 0, sizeof(*out));
+    out->kind = kind;
+    void* buf = nullptr;
+    GBK_CUDA(cudaMalloc(&buf, 4 * (size_t)std::max<int64_t>(n, 1) * nsources));
+    BatchOptions best = base_options(A, kind);
+    float best_ms = 1e30f;
+    int rc = GBK_SUCCESS;
+    if (kind == kBatchBfs) {
+        const int dirs[6] = {0, 0, 0, 0, 1, 2};
+        const int alphas[6] = {2, 4, 8, 14, 4, 4};
+        Batch* b = nullptr;
+        rc = cached_batch(A, kBatchBfs, base_options(A, kBatchBfs), &b, s);
+        BfsBatch* bb = static_cast<BfsBatch*>(b);
+        if (!rc) rc = bb->set_levels((int32_t*)buf, n, s);
+        for (int c = 0; c < 6 && !rc; ++c) {
+            rc = bb->set_mode(dirs[c], alphas[c], best.bfs_beta, s);
+            float ms = 0;
+            if (!rc) rc = time_one_shot(b, nsources, sources, nullptr, 0, false, s, &ms);
+            out->candidate_ms[c] = ms;
+            if (!rc && ms < best_ms) {
+                best_ms = ms;
+                best.bfs_direction = dirs[c];
+                best.bfs_alpha = alphas[c];
+            }
+        }
+        if (b) {
+            const int rc2 = bb->set_levels(nullptr, 0, s);
+            if (!rc) rc = rc2;
+        }
+        out->ncandidates = 6;
+    } else {
+        const int sizes[5] = {64, 128, 256, 512, 1024};
+        for (int c = 0; c < 5 && !rc; ++c) {
+            BatchOptions o = base_options(A, kind);
+            o.item_edges = sizes[c];
+            Batch* b = nullptr;
+            rc = kind == kBatchPpr ? make_ppr_batch(A, o, &b, s) : make_sssp_batch(A, o, &b, s);
+            float ms = 0;
+            if (!rc) rc = time_one_shot(b, nsources, sources, buf, n, true, s, &ms);
+            delete b;
+            out->candidate_ms[c] = ms;
+            if (!rc && ms < best_ms) {
+                best_ms = ms;
+                best.item_edges = sizes[c];
+            }
+        }
+        out->ncandidates = 5;
+    }
+    cudaFree(buf);
+    if (rc) return rc;
+    A->batch_tuned[kind] = true;
+    A->batch_tuned_opt[kind] = best;
+    out->item_edges = best.item_edges;
+    out->bfs_direction = best.bfs_direction;
+    out->bfs_alpha = best.bfs_alpha;
+    out->best_ms = best_ms;
+    return GBK_SUCCESS;
+}

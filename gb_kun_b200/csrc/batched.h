@@ -84,4 +84,7 @@ int make_sssp_batch(gbk_matrix A, const BatchOptions& o, Batch** out, cudaStream
 // BFS only: write levels straight into caller memory ([lane][stride]).
 int bfs_batch_set_levels(Batch* b, int32_t* levels, int64_t stride, cudaStream_t s);
 
+// The options gbk_batch_autotune chose for this matrix and kind, else the defaults.
+BatchOptions base_options(gbk_matrix A, int kind);
+
 }  // namespace gbk

@@ -71,6 +71,13 @@ int gbk_init(int device) {
     GBK_REQUIRE(p.major == 10, GBK_UNSUPPORTED, "gbk_init: device %d is sm_%d%d, this library is built for sm_100a",
                 device, p.major, p.minor);
     gbk::num_sms();
+    // Temporaries come from the stream-ordered pool; keep freed blocks in this
+    // process's pool instead of unmapping them at every synchronisation, which
+    // would make the next allocation of a vector-sized buffer map pages again.
+    cudaMemPool_t pool;
+    GBK_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = UINT64_MAX;
+    GBK_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     return GBK_SUCCESS;
 }
 

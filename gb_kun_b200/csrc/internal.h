@@ -70,6 +70,9 @@ struct gbk_matrix_s {
     // batches kept for the one-shot batched calls (BFS, PPR, SSSP)
     gbk::Batch* batch[3] = {nullptr, nullptr, nullptr};
     gbk::BatchOptions batch_opt[3];
+    // options chosen by gbk_batch_autotune, per kind
+    bool batch_tuned[3] = {false, false, false};
+    gbk::BatchOptions batch_tuned_opt[3];
 };
 
 namespace gbk {

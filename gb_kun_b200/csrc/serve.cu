@@ -120,9 +120,14 @@ int make_slot(gbk_server_s* S, int kind, Slot** out) {
         return cuda_fail(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
     }
     sl->s = s;
-    int rc = kind == kBatchBfs   ? make_bfs_batch(S->A, S->opt, &sl->b, s)
-             : kind == kBatchPpr ? make_ppr_batch(S->A, S->opt, &sl->b, s)
-                                 : make_sssp_batch(S->A, S->opt, &sl->b, s);
+    // the matrix's tuned options for this kind, with the server's PPR parameters
+    BatchOptions o = base_options(S->A, kind);
+    o.damping = S->opt.damping;
+    o.tol = S->opt.tol;
+    o.itermax = S->opt.itermax;
+    int rc = kind == kBatchBfs   ? make_bfs_batch(S->A, o, &sl->b, s)
+             : kind == kBatchPpr ? make_ppr_batch(S->A, o, &sl->b, s)
+                                 : make_sssp_batch(S->A, o, &sl->b, s);
     if (rc) {
         delete sl;
         return rc;

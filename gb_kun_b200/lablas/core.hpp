@@ -62,13 +62,20 @@ struct DeviceBuffer {
     DeviceBuffer(const DeviceBuffer&) = delete;
     DeviceBuffer& operator=(const DeviceBuffer&) = delete;
     ~DeviceBuffer() { release(); }
+    // stream-ordered: no device-wide synchronisation per temporary
     void alloc(size_t count) {
+        static const int ready = [] {  // once per process: gbk_init sets up the pool on the current device
+            int d = 0;
+            cudaGetDevice(&d);
+            return gbk_init(d);
+        }();
+        (void)ready;
         release();
         n = count;
-        cuda_check(cudaMalloc((void**)&p, sizeof(T) * (count ? count : 1)), "cudaMalloc");
+        cuda_check(cudaMallocAsync((void**)&p, sizeof(T) * (count ? count : 1), current_stream()), "cudaMallocAsync");
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, current_stream());
         p = nullptr;
         n = 0;
     }

@@ -192,6 +192,24 @@ int gbk_ppr(gbk_matrix A, const int32_t* seeds, int nseeds, double damping, doub
  * Synchronises the stream. */
 int gbk_sssp_multi(gbk_matrix A, const int32_t* sources, int nsources, int32_t* dist, int32_t* iters, void* stream);
 
+/* Tuning of the batched traversals on this graph: times each candidate on
+ * the given sources (CUDA events, best of 2 after a warm-up) and keeps the
+ * fastest for later gbk_msbfs / gbk_ppr / gbk_sssp_multi calls and servers
+ * on A.  kind: 0 BFS (candidates: push/pull switch factor 2, 4, 8, 14, push
+ * only, pull only), 1 PPR and 2 SSSP (edges per work item 64 .. 1024).  The
+ * reference has no tuner; it takes its format from the command line. */
+typedef struct gbk_batch_tune_result {
+    int32_t kind;
+    int32_t item_edges;     /* chosen edges per work item (PPR / SSSP) */
+    int32_t bfs_direction;  /* chosen BFS direction mode */
+    int32_t bfs_alpha;      /* chosen push -> pull switch factor */
+    int32_t ncandidates;
+    float best_ms;
+    float candidate_ms[8];
+} gbk_batch_tune_result;
+int gbk_batch_autotune(gbk_matrix A, int kind, const int32_t* sources, int nsources, gbk_batch_tune_result* out,
+                       void* stream);
+
 /* ---- vectors ------------------------------------------------------------ */
 
 /* Count of non-zero entries (DenseVector::get_nvals, dense_vector.hpp:44-52).
