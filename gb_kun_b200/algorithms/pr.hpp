@@ -68,6 +68,56 @@ inline void page_rank_sinks(Vector<float>* centrality, LAGraph_Graph<float>* G, 
     centrality->dup(rp);
 }
 
+// Personalised PageRank from one seed, built from the same lablas:: steps as
+// page_rank_sinks (one plus-second mxv per iteration): r0 = e_seed and the
+// teleport and sink mass return to the seed,
+//   r = [(1 - damping) + damping * sum_{sinks} r] e_seed + A (r ./ d),
+// stopping once sum |r_new - r| < tol (tol > 0) or after itermax iterations.
+// The sink mass is a plain sum over the zero-column-degree vertices (dense
+// vectors), not the reference's sparse-mask form.
+inline void personalized_page_rank(Vector<float>* centrality, LAGraph_Graph<float>* G, Index seed, int* iters,
+                                   int itermax = 100, double damping = 0.85, double tol = 1e-6) {
+    Matrix<float>* AT = G->AT;
+    Vector<Index>* d_out = G->coldegree;
+    Descriptor desc;
+    const Index n = AT->nrows();
+    const Vector<float>* NOMASK = nullptr;
+    float rdiff = 1;
+
+    Vector<float> t(n), r(n), w(n), d(n), d1(n), sinkf(n), tmp(n), tv(n);
+    Vector<float>* tp = &t;
+    Vector<float>* rp = &r;
+    assign(rp, NOMASK, GrB_NULL, 0.0f, GrB_ALL, n, (Descriptor*)nullptr);
+    rp->set_element(1.0f, seed);
+    assign(&tv, NOMASK, GrB_NULL, 0.0f, GrB_ALL, n, (Descriptor*)nullptr);
+    // 1.0 where the column degree is zero (complemented structural mask)
+    assign(&sinkf, NOMASK, GrB_NULL, 0.0f, GrB_ALL, n, (Descriptor*)nullptr);
+    assign(&sinkf, d_out, GrB_NULL, 1.0f, GrB_ALL, n, GrB_DESC_SC);
+    // d = max(d_out / damping, 1 / damping)
+    apply(&d, NOMASK, GrB_NULL, GrB_DIV_FP32, d_out, damping, &desc);
+    assign(&d1, NOMASK, GrB_NULL, (float)(1.0 / damping), GrB_ALL, n, (Descriptor*)nullptr);
+    eWiseAdd(&d, NOMASK, GrB_NULL, GrB_MAX_FP32, &d1, &d, (Descriptor*)nullptr);
+
+    for ((*iters) = 0; (*iters) < itermax; (*iters)++) {
+        if (tol > 0 && rdiff < tol) break;
+        eWiseMult(&tmp, NOMASK, GrB_NULL, multiplies<float>(), rp, &sinkf, (Descriptor*)nullptr);
+        float sink = 0;
+        reduce(&sink, GrB_NULL, GrB_PLUS_MONOID_FP32, &tmp, (Descriptor*)nullptr);
+        const float teleport = (float)((1.0 - damping) + damping * sink);
+        std::swap(tp, rp);  // t is the old score
+        eWiseMult(&w, NOMASK, GrB_NULL, GrB_DIV_FP32, tp, &d, (Descriptor*)nullptr);
+        assign(rp, NOMASK, GrB_NULL, 0.0f, GrB_ALL, n, (Descriptor*)nullptr);
+        mxv(rp, NOMASK, GrB_PLUS_FP32, LAGraph_plus_second_fp32, AT, &w, &desc);
+        tv.set_element(teleport, seed);
+        eWiseAdd(rp, NOMASK, GrB_NULL, GrB_PLUS_FP32, rp, &tv, (Descriptor*)nullptr);
+        assign(tp, NOMASK, GrB_MINUS_FP32, rp, GrB_ALL, n, (Descriptor*)nullptr);
+        apply(tp, NOMASK, GrB_NULL, GrB_ABS_FP32, tp, (Descriptor*)nullptr);
+        rdiff = 0;
+        reduce(&rdiff, GrB_NULL, GrB_PLUS_MONOID_FP32, tp, (Descriptor*)nullptr);
+    }
+    centrality->dup(rp);
+}
+
 }  // namespace algorithm
 }  // namespace lablas
 

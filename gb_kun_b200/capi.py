@@ -35,6 +35,17 @@ class GbkError(RuntimeError):
         self.status = status
 
 
+class BatchTuneResult(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("item_edges", C.c_int32), ("bfs_direction", C.c_int32),
+                ("bfs_alpha", C.c_int32), ("ncandidates", C.c_int32), ("best_ms", C.c_float),
+                ("candidate_ms", C.c_float * 8)]
+
+    def describe(self) -> dict:
+        return {"kind": ["bfs", "ppr", "sssp"][self.kind], "item_edges": self.item_edges,
+                "bfs_direction": self.bfs_direction, "bfs_alpha": self.bfs_alpha, "best_ms": round(self.best_ms, 3),
+                "candidate_ms": [round(x, 3) for x in list(self.candidate_ms)[:self.ncandidates]]}
+
+
 class FormatParams(C.Structure):
     _fields_ = [("sell_c", C.c_int32), ("sell_sigma", C.c_int32), ("seg_cols", C.c_int32),
                 ("lav_dense_frac", C.c_float), ("csr_kernel", C.c_int32), ("sell_hot_cols", C.c_int32),
@@ -111,6 +122,7 @@ def _declare(lib):
         "gbk_msbfs": ([vp, vp, ci, vp, ci, vp, vp], ci),
         "gbk_ppr": ([vp, vp, ci, C.c_double, C.c_double, ci, vp, vp, vp], ci),
         "gbk_sssp_multi": ([vp, vp, ci, vp, vp, vp], ci),
+        "gbk_batch_autotune": ([vp, ci, vp, ci, C.POINTER(BatchTuneResult), vp], ci),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name, None)
@@ -282,6 +294,15 @@ class Matrix:
         check(lib().gbk_sssp_multi(self.h, ptr(src), len(src), ptr(dist), ptr(iters), stream_ptr(stream)),
               "gbk_sssp_multi")
         return iters
+
+    def batch_autotune(self, kind: str, sources, stream=None) -> BatchTuneResult:
+        """Time the batched traversal candidates of `kind` ("bfs", "ppr", "sssp") on these sources
+        and keep the fastest for later batched calls and servers on this matrix."""
+        src = np.ascontiguousarray(sources, dtype=np.int32)
+        r = BatchTuneResult()
+        check(lib().gbk_batch_autotune(self.h, {"bfs": 0, "ppr": 1, "sssp": 2}[kind], ptr(src), len(src),
+                                       C.byref(r), stream_ptr(stream)), "gbk_batch_autotune")
+        return r
 
     def mxm_masked(self, A, B, semiring="plus_one", ctype=I32, stream=None):
         """C<self> = A (+.x) B with this matrix as the mask; returns a new Matrix."""

@@ -748,27 +748,14 @@ __device__ __forceinline__ void ppr_store_sum(float* r_out, int64_t row, float a
     if (mine) __stcs(r_out + row * 32 + (threadIdx.x & 31), acc);
 }
 
-// Per-block sums of the warps' lane partials, in warp order (deterministic).
-__device__ __forceinline__ void block_partials(double sink, double rd, double* out) {
-    __shared__ double s_sink[kBT / 32][32], s_rd[kBT / 32][32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    s_sink[warp][lane] = sink;
-    s_rd[warp][lane] = rd;
-    __syncthreads();
-    if (warp == 0) {
-        double a = 0, b = 0;
-        for (int w = 0; w < kBT / 32; ++w) {
-            a += s_sink[w][lane];
-            b += s_rd[w][lane];
-        }
-        out[lane] = a;
-        out[32 + lane] = b;
-    }
-}
+
+// Gathers of w rows each warp keeps in flight (latency x bandwidth needs
+// tens of KB per SM outstanding).
+constexpr int kPprInFlight = 8;
 
 // One warp per work item, lane k = column k.  An item is either a run of up
 // to 32 consecutive short rows or one piece of a long row; the warp loads 32
-// column ids at a time and keeps 8 gathers of 128-byte w rows in flight
+// column ids at a time and keeps kPprInFlight gathers of 128-byte w rows in flight
 // whatever the row lengths, closing each row when the edge index passes its
 // end (rows are summed in CSR order, as the reference's loop does).  Lanes of
 // inactive columns issue no loads.  Pieces of split rows park their sums for
@@ -783,6 +770,7 @@ __global__ void __launch_bounds__(kBT) k_ppr_spmm(const ColCfg* __restrict__ cfg
     const int32_t* __restrict__ rp = cfg->rp;
     const int32_t* __restrict__ col = cfg->col;
     const uint64_t pol = policy_evict_last();
+    const float* w_lane = w_in + lane;
     if (act) {
         const int64_t nitems = cfg->nitems;
         const int64_t gw = ((int64_t)blockIdx.x * kBT + threadIdx.x) >> 5;
@@ -797,15 +785,22 @@ __global__ void __launch_bounds__(kBT) k_ppr_spmm(const ColCfg* __restrict__ cfg
             for (int32_t e0 = eb; e0 < ee; e0 += 32) {
                 const int cnt = min(32, ee - e0);
                 const int32_t cl = lane < cnt ? __ldcs(col + e0 + lane) : 0;
-                for (int j = 0; j < cnt; j += 8) {
-                    float t[8];
+                for (int j = 0; j < cnt; j += kPprInFlight) {
+                    float t[kPprInFlight];
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) {
+                    for (int q = 0; q < kPprInFlight; ++q) {
                         const int32_t u = __shfl_sync(kFull, cl, (j + q) & 31);
-                        t[q] = (mine && j + q < cnt) ? ld_keep(w_in + (int64_t)u * 32 + lane, pol) : 0.f;
+                        t[q] = (mine && j + q < cnt) ? ld_keep(w_lane + ((int64_t)u << 5), pol) : 0.f;
+                    }
+                    // whole block inside the current row: plain adds (the
+                    // padding entries are +0, which leaves the sum unchanged)
+                    if (e0 + min(j + kPprInFlight, cnt) <= bound) {
+#pragma unroll
+                        for (int q = 0; q < kPprInFlight; ++q) acc += t[q];
+                        continue;
                     }
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) {
+                    for (int q = 0; q < kPprInFlight; ++q) {
                         if (j + q < cnt) {
                             const int32_t e = e0 + j + q;
                             while (e >= bound) {  // rows that end here (empty rows need no store)
@@ -837,42 +832,114 @@ __global__ void __launch_bounds__(kBT) k_ppr_fix(const ColCfg* __restrict__ cfg,
     const int64_t gw = ((int64_t)blockIdx.x * kBT + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * kBT) >> 5;
     for (int64_t i = gw; i < cfg->nsplit; i += nw) {
-        float acc = 0.f;
-        for (int32_t sl = cfg->split_first[i]; sl < cfg->split_first[i + 1]; ++sl)
-            acc += cfg->split_acc[(int64_t)sl * 32 + lane];
-        ppr_store_sum(r_out, cfg->split_row[i], acc, mine);
+        // four independent partial sums (slots k mod 4), added in a fixed order
+        float a[4] = {0.f, 0.f, 0.f, 0.f};
+        const int32_t s0 = cfg->split_first[i], s1 = cfg->split_first[i + 1];
+        int32_t sl = s0;
+        for (; sl + 4 <= s1; sl += 4) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) a[k] += cfg->split_acc[(int64_t)(sl + k) * 32 + lane];
+        }
+        for (int k = 0; sl < s1; ++sl, ++k) a[k] += cfg->split_acc[(int64_t)sl * 32 + lane];
+        ppr_store_sum(r_out, cfg->split_row[i], (a[0] + a[1]) + (a[2] + a[3]), mine);
     }
 }
 
-// Elementwise step over all n x 32 entries (coalesced, thread t always on
-// column t % 32): rank = row sum (0 for empty rows) plus the teleport at the
-// seed, w = rank / d, and the per-column partial sums of |rank - old| and of
-// the rank held by sinks, per block in a fixed order.
+// Elementwise step over all n x 32 entries, as float4 (thread t always on
+// columns 4 (t % 8) .. 4 (t % 8) + 3): rank = row sum (0 for empty rows) plus
+// the teleport at the seed, w = rank / d, and the per-column partial sums of
+// |rank - old| and of the rank held by sinks, per block in a fixed order.
+// Inactive columns are written back unchanged.
 __global__ void __launch_bounds__(kBT) k_ppr_update(const ColCfg* __restrict__ cfg, const PprState* __restrict__ st) {
+    __shared__ double s_sink[kBT / 32][32], s_rd[kBT / 32][32];
     const unsigned act = (unsigned)st->st.active;
-    const int lane = threadIdx.x & 31;
-    const bool mine = (act >> lane) & 1;
-    double sink = 0, rd = 0;
-    if (mine) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, quad = threadIdx.x & 7;
+    double sink[4] = {0, 0, 0, 0}, rd[4] = {0, 0, 0, 0};
+    if (act) {
+        bool m[4];
+        int32_t seed[4];
+        float tele[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            m[c] = (act >> (4 * quad + c)) & 1;
+            seed[c] = st->seed[4 * quad + c];
+            tele[c] = st->tele[4 * quad + c];
+        }
         const int cur = st->st.iter & 1;
-        const float* __restrict__ r_old = cfg->r[cur];
-        float* r_out = cfg->r[cur ^ 1];
-        float* w_out = cfg->w[cur ^ 1];
-        const int32_t seed = st->seed[lane];
-        const float tele = st->tele[lane];
+        const float4* __restrict__ r_old = (const float4*)cfg->r[cur];
+        float4* r_out = (float4*)cfg->r[cur ^ 1];
+        float4* w_out = (float4*)cfg->w[cur ^ 1];
         const int32_t* __restrict__ rp = cfg->rp;
-        const int64_t total = cfg->n * 32;
-        for (int64_t i = (int64_t)blockIdx.x * kBT + threadIdx.x; i < total; i += (int64_t)gridDim.x * kBT) {
-            const int64_t v = i >> 5;
-            const float acc = rp[v + 1] > rp[v] ? __ldcs(r_out + i) : 0.f;
-            const float rn = (v == seed) ? tele + acc : acc;
-            __stcs(r_out + i, rn);
-            __stcs(w_out + i, rn / cfg->d[v]);
-            rd += (double)fabsf(__ldcs(r_old + i) - rn);
-            if (cfg->cdeg[v] == 0) sink += (double)rn;
+        const int64_t total = cfg->n * 8;
+        const int64_t stride = (int64_t)gridDim.x * kBT;
+        constexpr int U = 2;
+        for (int64_t i0 = (int64_t)blockIdx.x * kBT + threadIdx.x; i0 < total; i0 += U * stride) {
+            float4 acc[U], old[U];
+            float dv[U];
+            int32_t cd[U];
+            bool ne[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                const int64_t i = i0 + k * stride;
+                if (i < total) {
+                    const int64_t v = i >> 3;
+                    ne[k] = rp[v + 1] > rp[v];
+                    acc[k] = __ldcs(r_out + i);
+                    old[k] = __ldcs(r_old + i);
+                    dv[k] = cfg->d[v];
+                    cd[k] = cfg->cdeg[v];
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                const int64_t i = i0 + k * stride;
+                if (i >= total) continue;
+                const int64_t v = i >> 3;
+                float a[4] = {acc[k].x, acc[k].y, acc[k].z, acc[k].w};
+                const float o[4] = {old[k].x, old[k].y, old[k].z, old[k].w};
+                float wv[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    if (m[c]) {
+                        const float x = ne[k] ? a[c] : 0.f;
+                        const float rn = (v == seed[c]) ? tele[c] + x : x;
+                        a[c] = rn;
+                        rd[c] += (double)fabsf(o[c] - rn);
+                        if (cd[k] == 0) sink[c] += (double)rn;
+                    }
+                    wv[c] = a[c] / dv[k];
+                }
+                __stcs(r_out + i, make_float4(a[0], a[1], a[2], a[3]));
+                __stcs(w_out + i, make_float4(wv[0], wv[1], wv[2], wv[3]));
+            }
         }
     }
-    block_partials(sink, rd, cfg->partial + (int64_t)blockIdx.x * 64);
+    // lanes l, l + 8, l + 16, l + 24 hold the same columns
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        for (int o = 8; o < 32; o <<= 1) {
+            sink[c] += __shfl_xor_sync(kFull, sink[c], o);
+            rd[c] += __shfl_xor_sync(kFull, rd[c], o);
+        }
+    }
+    if (lane < 8) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            s_sink[warp][4 * lane + c] = sink[c];
+            s_rd[warp][4 * lane + c] = rd[c];
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        double x = 0, y = 0;
+        for (int w2 = 0; w2 < kBT / 32; ++w2) {
+            x += s_sink[w2][lane];
+            y += s_rd[w2][lane];
+        }
+        double* out = cfg->partial + (int64_t)blockIdx.x * 64;
+        out[lane] = x;
+        out[32 + lane] = y;
+    }
 }
 
 // 1024 threads: thread (g, k) sums the parts g, g + 32, ... of column k, then

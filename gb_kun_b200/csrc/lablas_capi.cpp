@@ -194,6 +194,24 @@ int gbk_lablas_pagerank(gbk_lablas_graph g, int32_t itermax, double damping, dou
     });
 }
 
+int gbk_lablas_ppr(gbk_lablas_graph g, int64_t seed, int32_t itermax, double damping, double tol, float* ranks,
+                   int32_t* iterations, double* ms) {
+    if (!g || !ranks) return GBK_NULL_POINTER;
+    if (seed < 0 || seed >= g->n) return GBK_INVALID_INDEX;
+    return guarded([&] {
+        auto* A = g->unit_f();
+        LAGraph_Graph<float> graph(*A);
+        lablas::Vector<float> r(g->n);
+        int iters = 0;
+        Timer t(ms);
+        lablas::algorithm::personalized_page_rank(&r, &graph, (Index)seed, &iters, itermax, damping, tol);
+        t.stop();
+        if (iterations) *iterations = iters;
+        copy_out(r, ranks);
+        return 0;
+    });
+}
+
 int gbk_lablas_tc(gbk_lablas_graph g, uint64_t* count, double* ms) {
     if (!g || !count) return GBK_NULL_POINTER;
     return guarded([&] {

@@ -36,6 +36,7 @@ def lib():
         L.gbk_lablas_sssp_f32.argtypes = [vp, i64, vp, dp]
         L.gbk_lablas_sssp_i32.argtypes = [vp, i64, vp, dp]
         L.gbk_lablas_pagerank.argtypes = [vp, i32, C.c_double, C.c_double, vp, C.POINTER(i32), dp]
+        L.gbk_lablas_ppr.argtypes = [vp, i64, i32, C.c_double, C.c_double, vp, C.POINTER(i32), dp]
         L.gbk_lablas_tc.argtypes = [vp, C.POINTER(C.c_uint64), dp]
         L.gbk_lablas_spmv.argtypes = [vp, i32, vp, vp, vp, dp]
         _LIB = L
@@ -108,6 +109,14 @@ class Graph:
         ms = C.c_double()
         _check(lib().gbk_lablas_pagerank(self.h, itermax, damping, tol, _p(out), C.byref(it), C.byref(ms)),
                "pagerank")
+        return out, it.value, ms.value
+
+    def ppr(self, seed, itermax=100, damping=0.85, tol=1e-6):
+        out = np.empty(self.n, np.float32)
+        it = C.c_int32()
+        ms = C.c_double()
+        _check(lib().gbk_lablas_ppr(self.h, int(seed), itermax, damping, tol, _p(out), C.byref(it), C.byref(ms)),
+               "ppr")
         return out, it.value, ms.value
 
     def tc(self):

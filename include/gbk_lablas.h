@@ -40,6 +40,11 @@ int gbk_lablas_sssp_i32(gbk_lablas_graph g, int64_t source, int32_t* dist, doubl
  * itermax iterations or once rdiff < tol (tol > 0). */
 int gbk_lablas_pagerank(gbk_lablas_graph g, int32_t itermax, double damping, double tol, float* ranks,
                         int32_t* iterations, double* ms);
+/* Personalised PageRank from one seed through the same lablas:: steps
+ * (one plus-second mxv per iteration); teleport and sink mass return to the
+ * seed.  The single-query path the batched gbk_ppr is compared with. */
+int gbk_lablas_ppr(gbk_lablas_graph g, int64_t seed, int32_t itermax, double damping, double tol, float* ranks,
+                   int32_t* iterations, double* ms);
 /* Burkhardt triangle count (algorithms/tc/tc.hpp:209-217); the graph must be symmetric. */
 int gbk_lablas_tc(gbk_lablas_graph g, uint64_t* count, double* ms);
 /* y = A x through lablas::mxv (plus-times, f32) in the given storage format

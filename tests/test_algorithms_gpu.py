@@ -126,3 +126,16 @@ def test_lablas_spmv_vs_fp64(lc, oracle, fmt):
     x = gg.vector_f32(g.n, seed=2)
     y, _ = lc.Graph(g).spmv(val, x, fmt=fmt)
     assert rel_l1(y, oracle.spmv_f64(g, val, x)) < REL_L1_TOL
+
+
+@pytest.mark.parametrize("name,make", GRAPHS)
+def test_personalized_pagerank_vs_oracle(lc, oracle, name, make):
+    g = make()
+    G = lc.Graph(g)
+    for s in gg.sources(g, 3, seed=13):
+        r, it, _ = G.ppr(int(s), itermax=100, tol=1e-6)
+        want, _ = oracle.ppr(g, int(s), damping=0.85, tol=1e-6, itermax=100)
+        assert rel_l1(r, want) < REL_L1_TOL, (name, s)
+        r7, it7, _ = G.ppr(int(s), itermax=7, tol=0.0)
+        want7, _ = oracle.ppr(g, int(s), tol=0.0, itermax=7)
+        assert it7 == 7 and rel_l1(r7, want7) < REL_L1_TOL

@@ -175,3 +175,23 @@ def test_batched_rejects_bad_input(torch):
     assert e.value.status == 5
     # the matrix still works after the rejected calls
     A.msbfs(np.array([1], dtype=np.int32), lv[:1])
+
+
+def test_batch_autotune_keeps_results(torch, oracle):
+    _, g = GRAPHS[0]
+    A = _mat(g, val=gg.weights_i32(g, seed=3))
+    src = _sources(g, 64, seed=50)
+    rb = A.batch_autotune("bfs", src)
+    assert rb.ncandidates == 6 and rb.bfs_direction in (0, 1, 2) and rb.best_ms > 0
+    rp = A.batch_autotune("ppr", src[:32])
+    rs = A.batch_autotune("sssp", src[:32])
+    assert rp.item_edges in (64, 128, 256, 512, 1024) and rs.item_edges in (64, 128, 256, 512, 1024)
+    lv = torch.zeros((64, g.n), dtype=torch.int32, device="cuda")
+    A.msbfs(src, lv)
+    got = lv.cpu().numpy()
+    for k in (0, 40):
+        assert np.array_equal(got[k], oracle.bfs(g, int(src[k])))
+    r = torch.zeros((32, g.n), dtype=torch.float32, device="cuda")
+    A.ppr(src[:32], r)
+    want, _ = oracle.ppr(g, int(src[3]), tol=1e-6, itermax=100)
+    assert rel_l1(r[3].cpu().numpy(), want) < REL_L1_TOL
