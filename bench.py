@@ -552,6 +552,13 @@ def run_serve(args):
         res, wall = srv.run_trace(arr, kinds, srcs)
     launches = capi.launch_count() - l0
     burst, wall_b = srv.run_trace(np.zeros(nq), kinds, srcs)
+    # capacity per query kind (a burst of one kind only)
+    per_kind = {}
+    for k, name in ((0, "bfs"), (1, "ppr"), (2, "sssp")):
+        sel = np.flatnonzero(kinds == k)[:128]
+        if len(sel):
+            _, wk_s = srv.run_trace(np.zeros(len(sel)), kinds[sel], srcs[sel])
+            per_kind[name] = round(len(sel) / wk_s, 2)
     used, budget, nb = srv.memory()
     srv.close()
     # one query at a time through the same engine (one lane, nothing overlaps)
@@ -592,6 +599,7 @@ def run_serve(args):
                             "uniform over non-isolated vertices", "iters_per_launch": 4,
                    "l2": "graph and batch state larger than L2"},
         "latency_ms": lat, "qps_offered": args.rate, "qps_capacity_burst": round(cap, 2),
+        "qps_capacity_per_kind": per_kind,
         "batches": nb, "device_bytes_used": used, "memory_budget": budget,
         "one_at_a_time": {"qps_poisson": round(m / wall1, 2), "qps_capacity": round(cap1, 2),
                           "latency_ms": latency_stats(res1), "queries": m,
