@@ -14,6 +14,11 @@ stream, max over ranks).  Also reported: % of measured HBM peak, GTEPS
   python bench.py [--gpus N --steps K --warmup W] [--format CSR|SELL_C|CSR_SEG|LAV]
   python bench.py --impl reference   # the reference's OpenMP CPU SpMV, same config
 
+Other workloads, one JSON line each:
+  python bench.py --mode batched     # 64-source BFS, 32-column PPR / SSSP, R-MAT s22
+  python bench.py --mode serve       # Poisson BFS/SSSP/PPR requests on resident R-MAT s24
+  python bench.py --mode algorithms  # BFS/CC/PR/SSSP/TC on R-MAT s23 vs the reference CPU
+
 Multi-GPU: the hot path does not need an exchange at these sizes, so
 ``--gpus N`` (under torchrun) runs N independent replicas, one per GPU, and
 ``value`` sums their work ("scaling": "weak").
@@ -520,7 +525,7 @@ def run_batched(args):
         "roofline": {"bound": "hbm", "kernel": "k_ppr_spmm (+ k_ppr_fix, k_ppr_control); bytes per iteration "
                                                "4(n+1) + 4 nnz + 2*n*32*4",
                      "achieved": round(spmm_gbs, 2), "peak": peak, "unit": "GB/s", "frac": round(spmm_gbs / peak, 4),
-                     "traffic": None},
+                     "traffic": read_traffic("batched_traversals_rmat22") if args.scale == 22 else None},
         "e2e": {"value": round(edges / (e2e_ms * 1e-3) / 1e9, 3), "unit": "GTEPS", "h2d_bytes_per_step": 4 * 64,
                 "d2h_bytes_per_step": 4 * 64 * g.n, "ms_per_step": round(e2e_ms, 3)},
         "gpu_launches": int(launches), "clocks": clk.summary(), "cpu_baseline": cpu,

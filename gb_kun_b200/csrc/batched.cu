@@ -11,7 +11,9 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <vector>
 
 #include "batched.h"
@@ -41,20 +43,30 @@ __device__ __forceinline__ unsigned long long warp_sum64(unsigned long long x) {
     return x;
 }
 
+using LoopBody = std::function<int(cudaStream_t, cudaGraphConditionalHandle)>;
+
 // A graph whose only root node is a `while` conditional; its body is one
-// iteration, captured from a stream.
+// iteration, captured from a stream.  With GBK_BATCH_HOST_LOOP=1 in the
+// environment (for profilers that do not follow conditional graph nodes) the
+// same body kernels are launched from a host loop instead, one iteration per
+// round trip, stopping by the rules the control kernels apply.
 struct LoopGraph {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaGraphConditionalHandle handle = 0;
+    LoopBody body;
+    bool host = false;
     ~LoopGraph() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
     }
 };
 
-template <typename Body>
-int build_loop(LoopGraph& g, Body&& body) {
+int build_loop(LoopGraph& g, LoopBody body) {
+    g.body = std::move(body);
+    const char* env = getenv("GBK_BATCH_HOST_LOOP");
+    g.host = env && env[0] == '1';
+    if (g.host) return GBK_SUCCESS;
     GBK_CUDA(cudaGraphCreate(&g.graph, 0));
     GBK_CUDA(cudaGraphConditionalHandleCreate(&g.handle, g.graph, 1, cudaGraphCondAssignDefault));
     cudaGraphNodeParams p = {};
@@ -72,13 +84,34 @@ int build_loop(LoopGraph& g, Body&& body) {
         cudaStreamDestroy(cs);
         return cuda_fail(e, "cudaStreamBeginCaptureToGraph", __FILE__, __LINE__);
     }
-    const int rc = body(cs, g.handle);
+    const int rc = g.body(cs, g.handle);
     cudaGraph_t captured = nullptr;
     e = cudaStreamEndCapture(cs, &captured);
     cudaStreamDestroy(cs);
     if (rc) return rc;
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
     GBK_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+    return GBK_SUCCESS;
+}
+
+// One launch of the loop; the status lands in h_status on stream s.
+int run_loop(LoopGraph& g, BatchStatus* d_status, BatchStatus* h_status, int budget, bool stop_on_finish,
+             cudaStream_t s) {
+    if (!g.host) {
+        GBK_CUDA(cudaGraphLaunch(g.exec, s));
+        GBK_CUDA(cudaMemcpyAsync(h_status, d_status, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
+        return GBK_SUCCESS;
+    }
+    GBK_CUDA(cudaMemcpyAsync(h_status, d_status, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
+    GBK_CUDA(cudaStreamSynchronize(s));
+    const unsigned long long fin0 = h_status->finished;
+    for (int i = 0; i < budget && h_status->active; ++i) {
+        const int rc = g.body(s, 0);
+        if (rc) return rc;
+        GBK_CUDA(cudaMemcpyAsync(h_status, d_status, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
+        GBK_CUDA(cudaStreamSynchronize(s));
+        if (stop_on_finish && (h_status->finished & ~fin0)) break;
+    }
     return GBK_SUCCESS;
 }
 
@@ -617,7 +650,7 @@ struct BfsBatch final : Batch {
         grid_push = persistent_blocks((const void*)k_bfs_push, kBT);
         grid_pull = persistent_blocks((const void*)k_bfs_pull, kBT);
         grid_fin = persistent_blocks((const void*)k_bfs_finalize, kBT);
-        return build_loop(loop, [&](cudaStream_t cs, cudaGraphConditionalHandle h) -> int {
+        return build_loop(loop, [this, n](cudaStream_t cs, cudaGraphConditionalHandle h) -> int {
             k_bfs_push<<<grid_push, kBT, 0, cs>>>(d_cfg, d_st);
             GBK_LAUNCH_CHECK();
             k_bfs_pull<<<grid_pull, kBT, 0, cs>>>(d_cfg, d_st);
@@ -669,9 +702,7 @@ struct BfsBatch final : Batch {
     int launch(int budget, bool stop_on_finish, cudaStream_t s) override {
         k_set_launch<BfsState><<<1, 1, 0, s>>>(d_st, budget, stop_on_finish ? 1 : 0);
         GBK_LAUNCHED();
-        GBK_CUDA(cudaGraphLaunch(loop.exec, s));
-        GBK_CUDA(cudaMemcpyAsync(h_st, &d_st->st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
-        return GBK_SUCCESS;
+        return run_loop(loop, &d_st->st, h_st, budget, stop_on_finish, s);
     }
 
     int extract(int lane_lo, int nl, void* dst, int64_t stride, cudaStream_t s) override {
@@ -1145,7 +1176,7 @@ struct PprBatch final : Batch {
         GBK_CUDA(cudaMemcpyAsync(d_st, &init, sizeof(PprState), cudaMemcpyHostToDevice, s));
         GBK_CUDA(cudaStreamSynchronize(s));
         bytes = 8 * nn + 4 * 4 * 32 * nn + 4 * 32 * (size_t)items.nslots + 20 * (size_t)items.nitems;
-        return build_loop(loop, [&](cudaStream_t cs, cudaGraphConditionalHandle h) -> int {
+        return build_loop(loop, [this](cudaStream_t cs, cudaGraphConditionalHandle h) -> int {
             k_ppr_spmm<<<grid_main, kBT, 0, cs>>>(d_cfg, d_st);
             GBK_LAUNCH_CHECK();
             k_ppr_fix<<<grid_fix, kBT, 0, cs>>>(d_cfg, d_st);
@@ -1186,9 +1217,7 @@ struct PprBatch final : Batch {
     int launch(int budget, bool stop_on_finish, cudaStream_t s) override {
         k_set_launch<PprState><<<1, 1, 0, s>>>(d_st, budget, stop_on_finish ? 1 : 0);
         GBK_LAUNCHED();
-        GBK_CUDA(cudaGraphLaunch(loop.exec, s));
-        GBK_CUDA(cudaMemcpyAsync(h_st, &d_st->st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
-        return GBK_SUCCESS;
+        return run_loop(loop, &d_st->st, h_st, budget, stop_on_finish, s);
     }
 
     int extract(int lane_lo, int nl, void* dst, int64_t stride, cudaStream_t s) override {
@@ -1394,7 +1423,7 @@ struct SsspBatch final : Batch {
         GBK_CUDA(cudaMemcpyAsync(d_st, &init, sizeof(SsspState), cudaMemcpyHostToDevice, s));
         GBK_CUDA(cudaStreamSynchronize(s));
         bytes = 4 * 32 * nn + 8 * nn + 20 * (size_t)items.nitems;
-        return build_loop(loop, [&](cudaStream_t cs, cudaGraphConditionalHandle h) -> int {
+        return build_loop(loop, [this](cudaStream_t cs, cudaGraphConditionalHandle h) -> int {
             k_sssp_push<<<grid_main, kBT, 0, cs>>>(d_cfg, d_st);
             GBK_LAUNCH_CHECK();
             k_sssp_finalize<<<grid_fin, kBT, 0, cs>>>(d_cfg, d_st);
@@ -1433,9 +1462,7 @@ struct SsspBatch final : Batch {
     int launch(int budget, bool stop_on_finish, cudaStream_t s) override {
         k_set_launch<SsspState><<<1, 1, 0, s>>>(d_st, budget, stop_on_finish ? 1 : 0);
         GBK_LAUNCHED();
-        GBK_CUDA(cudaGraphLaunch(loop.exec, s));
-        GBK_CUDA(cudaMemcpyAsync(h_st, &d_st->st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
-        return GBK_SUCCESS;
+        return run_loop(loop, &d_st->st, h_st, budget, stop_on_finish, s);
     }
 
     int extract(int lane_lo, int nl, void* dst, int64_t stride, cudaStream_t s) override {

@@ -195,3 +195,37 @@ def test_batch_autotune_keeps_results(torch, oracle):
     A.ppr(src[:32], r)
     want, _ = oracle.ppr(g, int(src[3]), tol=1e-6, itermax=100)
     assert rel_l1(r[3].cpu().numpy(), want) < REL_L1_TOL
+
+
+_HOST_LOOP_SCRIPT = r"""
+import sys, numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+from gb_kun_b200 import capi, graphgen as gg
+capi.init(0)
+g = gg.rmat(11, 16, seed=7)
+A = capi.Matrix.from_graph(g, val=gg.weights_i32(g, seed=3))
+src = gg.sources(g, 32, seed=60).astype(np.int32)
+lv = torch.zeros((32, g.n), dtype=torch.int32, device="cuda"); A.msbfs(src, lv)
+r = torch.zeros((32, g.n), dtype=torch.float32, device="cuda"); A.ppr(src, r)
+d = torch.zeros((32, g.n), dtype=torch.int32, device="cuda"); A.sssp_multi(src, d)
+np.savez(sys.argv[2], lv=lv.cpu().numpy(), r=r.cpu().numpy(), d=d.cpu().numpy())
+"""
+
+
+def test_host_loop_mode_matches_graph_mode(torch, tmp_path):
+    """GBK_BATCH_HOST_LOOP=1 (for profilers) runs the same iteration kernels from the host."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parent.parent
+    outs = {}
+    for mode in ("0", "1"):
+        f = tmp_path / f"m{mode}.npz"
+        env = dict(os.environ, GBK_BATCH_HOST_LOOP=mode)
+        res = subprocess.run([sys.executable, "-c", _HOST_LOOP_SCRIPT, str(root), str(f)], env=env,
+                             capture_output=True, text=True, timeout=300)
+        assert res.returncode == 0, res.stderr[-2000:]
+        outs[mode] = np.load(f)
+    for k in ("lv", "r", "d"):
+        assert np.array_equal(outs["0"][k], outs["1"][k]), k
