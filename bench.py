@@ -74,6 +74,8 @@ def parse():
     p.add_argument("--serial-queries", type=int, default=60, help="serve: requests run one at a time")
     p.add_argument("--serve-scale", type=int, default=24, help="serve: R-MAT scale of the resident graph")
     p.add_argument("--alg-scale", type=int, default=23, help="algorithms: R-MAT scale")
+    p.add_argument("--no-extras", action="store_true",
+                   help="default line without the batched / served summaries (SpMV only)")
     return p.parse_args()
 
 
@@ -407,6 +409,8 @@ def run_ours(args):
         out["cpu_baseline"] = cpu_baseline(args, g, val, x)
     if args.sweep and rank == 0:
         out["format_sweep"] = format_sweep(args, peak)
+    if rank == 0 and world == 1 and not args.no_extras:
+        out.update(extras_summary(args))
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
@@ -530,7 +534,7 @@ def run_batched(args):
                 "d2h_bytes_per_step": 4 * 64 * g.n, "ms_per_step": round(e2e_ms, 3)},
         "gpu_launches": int(launches), "clocks": clk.summary(), "cpu_baseline": cpu,
     }
-    print(json.dumps(out), flush=True)
+    return out
 
 
 def run_serve(args):
@@ -615,7 +619,38 @@ def run_serve(args):
                 "d2h_bytes_per_step": 24, "note": "requests enter and summaries leave through the host loop"},
         "gpu_launches": int(launches), "clocks": clk.summary(), "graph_gen_s": round(t_gen, 1),
     }
-    print(json.dumps(out), flush=True)
+    return out
+
+
+def extras_summary(args):
+    """Compact batched and served results for the default line (each guarded:
+    a failure there is reported, the SpMV line still prints)."""
+    res = {}
+    try:
+        b = run_batched(args)
+        res["batched"] = {"workload": b["config"]["workload"], "msbfs64_ms": b["msbfs"]["ms"],
+                          "msbfs64_gteps": b["value"], "msbfs_speedup_vs_one_at_a_time":
+                              b["msbfs"]["speedup_vs_one_at_a_time"],
+                          "ppr32_ms": b["ppr"]["ms"], "ppr_rel_l1_vs_fp64": b["ppr"]["rel_l1_vs_fp64_lane0"],
+                          "sssp32_ms": b["sssp"]["ms"], "sssp_speedup_vs_one_at_a_time":
+                              b["sssp"]["speedup_vs_one_at_a_time"],
+                          "bit_exact_checked": b["msbfs"]["bit_exact_checked"] and b["sssp"]["bit_exact_checked"],
+                          "autotuned": b["config"]["autotuned"]}
+    except Exception as e:  # reported, never fatal for the SpMV number
+        res["batched"] = {"error": str(e)[:300]}
+    try:
+        v = run_serve(args)
+        o = v["one_at_a_time"]
+        res["served"] = {"workload": v["config"]["workload"], "qps": v["value"], "p50_ms": v["latency_ms"]["p50_ms"],
+                         "p99_ms": v["latency_ms"]["p99_ms"], "qps_capacity": v["qps_capacity_burst"],
+                         "qps_capacity_per_kind": v["qps_capacity_per_kind"],
+                         "one_at_a_time_qps_same_engine": o["qps_capacity"],
+                         "one_at_a_time_qps_best_single_query_path": o["qps_capacity_best_single_query_path"],
+                         "speedup_vs_same_engine_one_at_a_time": round(v["qps_capacity_burst"] / o["qps_capacity"], 2),
+                         "speedup_vs_best_single_query_path": v["speedup_qps_vs_one_at_a_time"]}
+    except Exception as e:
+        res["served"] = {"error": str(e)[:300]}
+    return res
 
 
 def run_algorithms(args):
@@ -691,7 +726,7 @@ def run_algorithms(args):
                                                 "cores": R.max_threads(), "kind": "reference",
                                                 "sample": "one run per algorithm on the same graph"},
     }
-    print(json.dumps(out), flush=True)
+    return out
 
 
 def run_reference(args):
@@ -727,7 +762,8 @@ def run_reference(args):
 def main():
     args = parse()
     if args.mode != "spmv":
-        {"batched": run_batched, "serve": run_serve, "algorithms": run_algorithms}[args.mode](args)
+        out = {"batched": run_batched, "serve": run_serve, "algorithms": run_algorithms}[args.mode](args)
+        print(json.dumps(out), flush=True)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -27,7 +27,10 @@ namespace gbk {
 namespace {
 
 constexpr int kBinThreads = 256;
-constexpr int kSplitNnz = 2048;
+#ifndef GBK_SPLIT_NNZ
+#define GBK_SPLIT_NNZ 2048
+#endif
+constexpr int kSplitNnz = GBK_SPLIT_NNZ;
 // bins: 0 empty, 1..6 -> G = 1,2,4,8,16,32, 7 warp, 8 split
 constexpr int kNumBins = 9;
 constexpr int kBinWarp = 7;
