@@ -32,6 +32,7 @@ CU_SOURCES = [
     "spmv_csr.cu",
     "spmv_bins.cu",
     "spmv_formats.cu",
+    "spmv_segsmem.cu",
     "spmspv.cu",
     "vector_ops.cu",
     "spgemm.cu",

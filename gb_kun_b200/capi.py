@@ -49,7 +49,7 @@ class BatchTuneResult(C.Structure):
 class FormatParams(C.Structure):
     _fields_ = [("sell_c", C.c_int32), ("sell_sigma", C.c_int32), ("seg_cols", C.c_int32),
                 ("lav_dense_frac", C.c_float), ("csr_kernel", C.c_int32), ("sell_hot_cols", C.c_int32),
-                ("sell_reorder_cols", C.c_int32)]
+                ("sell_reorder_cols", C.c_int32), ("seg_staged", C.c_int32)]
 
 
 class MatrixInfo(C.Structure):
@@ -225,11 +225,11 @@ class Matrix:
         return inf
 
     def set_format(self, fmt: str, sell_c=0, sigma=0, seg_cols=0, lav_frac=0.0, csr_kernel=0, hot_cols=0,
-                   reorder_cols=0, stream=None):
+                   reorder_cols=0, seg_staged=0, stream=None):
         """Storage format; csr_kernel picks the CSR kernel (0 default bins, 1 merge-path, 2 bins);
         hot_cols > 0 stages the x values of the most used columns in shared memory (SELL-C);
         reorder_cols renumbers columns by in-degree (SELL-C)."""
-        p = FormatParams(sell_c, sigma, seg_cols, lav_frac, csr_kernel, hot_cols, reorder_cols)
+        p = FormatParams(sell_c, sigma, seg_cols, lav_frac, csr_kernel, hot_cols, reorder_cols, seg_staged)
         check(lib().gbk_matrix_set_format(self.h, FMT[fmt], C.byref(p), stream_ptr(stream)), "gbk_matrix_set_format")
 
     def autotune(self, transpose=False, semiring="plus_times", reps=20, stream=None) -> TuneResult:

@@ -115,67 +115,67 @@ template <int SR, typename T> struct Semiring;
 
 template <typename T> struct Semiring<GBK_PLUS_TIMES, T> {
     static constexpr bool assoc = true;
-    __device__ static T identity() { return T(0); }
+    __host__ __device__ static T identity() { return T(0); }
     __device__ static T add(T a, T b) { return elem_add(a, b); }
     __device__ static T mul(T a, T x) { return a * x; }
 };
 template <typename T> struct Semiring<GBK_LOR_LAND, T> {
     static constexpr bool assoc = true;
-    __device__ static T identity() { return T(0); }
+    __host__ __device__ static T identity() { return T(0); }
     __device__ static T add(T a, T b) { return (a != T(0) || b != T(0)) ? T(1) : T(0); }
     __device__ static T mul(T a, T x) { return (a != T(0) && x != T(0)) ? T(1) : T(0); }
 };
 template <typename T> struct Semiring<GBK_FIRST_WINS, T> {  // first() is not associative with 0
     static constexpr bool assoc = false;
-    __device__ static T identity() { return T(0); }
+    __host__ __device__ static T identity() { return T(0); }
     __device__ static T add(T a, T b) { return a; }
     __device__ static T mul(T a, T x) { return a * x; }
 };
 template <typename T> struct Semiring<GBK_FIRST_MIN, T> {
     static constexpr bool assoc = true;
-    __device__ static T identity() { return T(0); }
+    __host__ __device__ static T identity() { return T(0); }
     __device__ static T add(T a, T b) { return b < a ? b : a; }
     __device__ static T mul(T a, T x) { return a * x; }
 };
 template <typename T> struct Semiring<GBK_PLUS_SECOND, T> {
     static constexpr bool assoc = true;
-    __device__ static T identity() { return T(0); }
+    __host__ __device__ static T identity() { return T(0); }
     __device__ static T add(T a, T b) { return elem_add(a, b); }
     __device__ static T mul(T, T x) { return x; }
 };
 template <typename T> struct Semiring<GBK_STRUCTURAL_BOOL, T> {
     static constexpr bool assoc = true;
-    __device__ static T identity() { return T(0); }
+    __host__ __device__ static T identity() { return T(0); }
     __device__ static T add(T a, T b) { return (a != T(0) || b != T(0)) ? T(1) : T(0); }
     __device__ static T mul(T, T) { return T(1); }
 };
 template <typename T> struct Semiring<GBK_MIN_PLUS, T> {
     static constexpr bool assoc = true;
-    __device__ static T identity() { return Lim<T>::max(); }
+    __host__ __device__ static T identity() { return Lim<T>::max(); }
     __device__ static T add(T a, T b) { return b < a ? b : a; }
     __device__ static T mul(T a, T x) { return elem_add(a, x); }
 };
 template <typename T> struct Semiring<GBK_CUSTOM_LESS_PLUS, T> {  // less() is not associative
     static constexpr bool assoc = false;
-    __device__ static T identity() { return Lim<T>::max(); }
+    __host__ __device__ static T identity() { return Lim<T>::max(); }
     __device__ static T add(T a, T b) { return a < b ? T(1) : T(0); }
     __device__ static T mul(T a, T x) { return elem_add(a, x); }
 };
 template <typename T> struct Semiring<GBK_MIN_SECOND, T> {
     static constexpr bool assoc = true;
-    __device__ static T identity() { return Lim<T>::max(); }
+    __host__ __device__ static T identity() { return Lim<T>::max(); }
     __device__ static T add(T a, T b) { return b < a ? b : a; }
     __device__ static T mul(T, T x) { return x; }
 };
 template <typename T> struct Semiring<GBK_MIN_NOTEQ, T> {
     static constexpr bool assoc = true;
-    __device__ static T identity() { return Lim<T>::max(); }
+    __host__ __device__ static T identity() { return Lim<T>::max(); }
     __device__ static T add(T a, T b) { return b < a ? b : a; }
     __device__ static T mul(T a, T x) { return a != x ? T(1) : T(0); }
 };
 template <typename T> struct Semiring<GBK_PLUS_ONE, T> {
     static constexpr bool assoc = true;
-    __device__ static T identity() { return T(0); }
+    __host__ __device__ static T identity() { return T(0); }
     __device__ static T add(T a, T b) { return elem_add(a, b); }
     __device__ static T mul(T, T) { return T(1); }
 };

@@ -38,6 +38,7 @@ struct CsrView {
 
 struct SellC;     // spmv_formats.cu
 struct SegCsr;    // spmv_formats.cu (CSR_SEG and LAV share one layout)
+struct SegSmem;   // spmv_segsmem.cu (CSR_SEG with x windows staged in shared memory)
 struct Batch;     // batched.h
 
 // Tunables of the batched traversals (batched.cu).
@@ -64,6 +65,7 @@ struct gbk_matrix_s {
     gbk::SellC* sell[2] = {nullptr, nullptr};
     gbk::SegCsr* seg[2] = {nullptr, nullptr};
     gbk::SegCsr* lav[2] = {nullptr, nullptr};
+    gbk::SegSmem* segx[2] = {nullptr, nullptr};
     void* xcopy = nullptr;      // n elements, used when x aliases y
     int64_t xcopy_elems = 0;
     int device = 0;
@@ -98,6 +100,13 @@ int spmv_format(gbk_matrix A, int transpose, int sr, int accum, int dtype, const
                 cudaStream_t s);
 int build_format(gbk_matrix A, gbk_format fmt, const gbk_format_params* p, cudaStream_t s);
 size_t format_bytes(gbk_matrix A);
+
+// CSR_SEG with staged x windows (spmv_segsmem.cu).  run_segsmem returns
+// GBK_UNSUPPORTED for semirings whose add it cannot fold atomically.
+int build_segsmem(const CsrView& a, int dtype, SegSmem** out, cudaStream_t s);
+int run_segsmem(const SegSmem* f, int sr, int accum, int dtype, const void* x, void* y, cudaStream_t s);
+void free_segsmem(SegSmem* f);
+size_t segsmem_bytes(const SegSmem* f);
 int64_t format_padded_nnz(gbk_matrix A);
 
 }  // namespace gbk

@@ -1023,6 +1023,12 @@ int format_dispatch(gbk_matrix A, int orient, int sr, int accum, const T* x, T* 
 int spmv_format(gbk_matrix A, int transpose, int sr, int accum, int dtype, const void* x, void* y,
                 cudaStream_t s) {
     const int orient = transpose ? 1 : 0;
+    if (A->format == GBK_FMT_CSR_SEG && A->segx[orient]) {
+        const int rc = run_segsmem(A->segx[orient], sr, accum, dtype, x, y, s);
+        if (rc != GBK_UNSUPPORTED) return rc;
+        // add operators that cannot be folded atomically: the CSR kernels
+        return spmv_csr(orient ? A->csc : A->csr, sr, accum, dtype, x, y, nullptr, 0, 0, s);
+    }
     if (dtype == GBK_F32) return format_dispatch<float>(A, orient, sr, accum, (const float*)x, (float*)y, s);
     return format_dispatch<int32_t>(A, orient, sr, accum, (const int32_t*)x, (int32_t*)y, s);
 }
@@ -1032,6 +1038,8 @@ int free_formats(gbk_matrix A) {
         free_sell(A->sell[o]);
         free_seg(A->seg[o]);
         free_seg(A->lav[o]);
+        free_segsmem(A->segx[o]);
+        A->segx[o] = nullptr;
         A->sell[o] = nullptr;
         A->seg[o] = nullptr;
         A->lav[o] = nullptr;
@@ -1056,6 +1064,8 @@ int build_format(gbk_matrix A, gbk_format fmt, const gbk_format_params* p, cudaS
                 GBK_INVALID_VALUE, "bad format parameters");
     GBK_REQUIRE(prm.csr_kernel >= 0 && prm.csr_kernel <= kKernelBins, GBK_INVALID_VALUE, "bad csr_kernel %d",
                 prm.csr_kernel);
+    GBK_REQUIRE(prm.seg_staged >= -1 && prm.seg_staged <= 1, GBK_INVALID_VALUE, "bad seg_staged %d",
+                prm.seg_staged);
     free_formats(A);
     A->params = prm;
     A->csr.kernel = prm.csr_kernel;
@@ -1072,6 +1082,8 @@ int build_format(gbk_matrix A, gbk_format fmt, const gbk_format_params* p, cudaS
                      ? build_sell<float>(v, prm.sell_sigma, prm.sell_hot_cols, prm.sell_reorder_cols, &A->sell[o], s)
                      : build_sell<int32_t>(v, prm.sell_sigma, prm.sell_hot_cols, prm.sell_reorder_cols, &A->sell[o],
                                            s);
+        } else if (fmt == GBK_FMT_CSR_SEG && prm.seg_staged >= 0) {
+            rc = build_segsmem(v, A->vtype, &A->segx[o], s);
         } else if (fmt == GBK_FMT_CSR_SEG) {
             rc = A->vtype == GBK_F32 ? build_seg<float>(v, prm.seg_cols, &A->seg[o], s)
                                      : build_seg<int32_t>(v, prm.seg_cols, &A->seg[o], s);
@@ -1094,6 +1106,7 @@ size_t format_bytes(gbk_matrix A) {
             b += f->padded * (4 + eb) + f->nslices * 12 + f->n * 4 + f->nov * (4 + eb);
             b += f->ov.nnz * (4 + eb) + (f->ov.nrows + 1) * 4;
         }
+        b += segsmem_bytes(A->segx[o]);
         const SegCsr* g = A->seg[o] ? A->seg[o] : A->lav[o];
         if (g) b += g->v.nnz * (4 + eb) + (g->nvrows + 1) * 4 * 2 + (g->n + 1) * 4 + g->nvrows * eb;
     }

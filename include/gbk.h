@@ -39,6 +39,9 @@ typedef struct gbk_format_params {
                                 0 = off; at most 53248 */
     int32_t sell_reorder_cols; /* SELL-C: renumber columns by in-degree (most used first) so gathers of
                                   popular x values share sectors and L1 lines; implied by sell_hot_cols */
+    int32_t seg_staged;      /* CSR_SEG: 0 (default) windows of 49152 columns whose x values are staged in
+                                shared memory, row sums folded into y atomically; -1 = seg_cols-wide
+                                segments gathered from L2 and merged per row in segment order */
 } gbk_format_params;
 
 /* A mask argument: either dense (n entries of `dtype`, non-zero = set) or

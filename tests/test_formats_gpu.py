@@ -36,13 +36,16 @@ GRAPHS = {
 }
 
 FORMATS = [("SELL_C", 1), ("SELL_C", 256), ("SELL_C", 4096), ("SELL_C_HOT", 4096), ("SELL_C_HOT", 1), ("CSR_SEG", 0),
-           ("LAV", 0)]
+           ("CSR_SEG_MERGE", 0), ("LAV", 0)]
 
 
 def apply(A, fmt, sigma, seg_cols):
-    """SELL_C_HOT: SELL-C with 1024 shared-memory x columns."""
+    """SELL_C_HOT: SELL-C with 1024 shared-memory x columns; CSR_SEG is the
+    staged-window kernel, CSR_SEG_MERGE the unstaged segments with a merge."""
     if fmt == "SELL_C_HOT":
         A.set_format("SELL_C", sigma=sigma, hot_cols=1024)
+    elif fmt == "CSR_SEG_MERGE":
+        A.set_format("CSR_SEG", seg_cols=seg_cols, seg_staged=-1)
     else:
         A.set_format(fmt, sigma=sigma, seg_cols=seg_cols if fmt != "SELL_C" else 0)
 
@@ -126,3 +129,34 @@ def test_masked_call_uses_csr_semantics(capi, oracle):
     y = dev(y0)
     A.mxv(dev(x), y, semiring="lor_land", mask=dev(m), mask_mode="str_comp")
     assert np.array_equal(y.cpu().numpy(), oracle.mxv("lor_land", g, val, x, y0, mask=m, mask_mode=5))
+
+
+@pytest.mark.parametrize("sr", ["plus_times", "min_plus", "lor_land", "plus_one", "min_second", "first_wins"])
+@pytest.mark.parametrize("accum", ["second", "plus"])
+def test_staged_segments_many_windows(capi, oracle, sr, accum):
+    """CSR_SEG with x windows in shared memory on a graph of 3 windows (131072
+    columns), every add class (atomic add / min / or) and the CSR fallback
+    for a non-associative add; float sums within REL_L1_TOL, integers exact."""
+    g = gg.rmat(17, 12, seed=8)
+    if sr == "plus_times":
+        val = gg.values_f32(g, seed=1)
+        x = gg.vector_f32(g.n, seed=2)
+        y0 = np.full(g.n, 0.5, np.float32)
+    else:
+        val = gg.weights_i32(g, seed=3, lo=1, hi=100)
+        x = (gg.vector_f32(g.n, seed=4) * 1000).astype(np.int32)
+        x[::5] = 0
+        y0 = np.full(g.n, 7, np.int32)
+    A = capi.Matrix.from_graph(g, val)
+    A.set_format("CSR_SEG")
+    for transpose in (False, True):
+        y = dev(y0.copy())
+        A.mxv(dev(x), y, semiring=sr, accum=accum, transpose=transpose)
+        go, vo = transposed(oracle, g, val) if transpose else (g, val)
+        acc_code = {"second": 0, "plus": 2}[accum]
+        expect = oracle.mxv(sr, go, vo, x, y0.copy(), accum=acc_code)
+        got = y.cpu().numpy()
+        if sr == "plus_times":
+            assert rel_l1(got, expect) < REL_L1_TOL, (transpose, rel_l1(got, expect))
+        else:
+            assert np.array_equal(got, expect), (sr, accum, transpose)
