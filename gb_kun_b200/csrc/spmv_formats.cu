@@ -37,6 +37,10 @@ constexpr int kSellMaxLen = 1 << 30;  // long slices are cut into work items ins
 constexpr int kSellChunk = 64;        // slice steps per work item (one warp)
 constexpr int kSellUnroll = 8;        // steps per pipelined load group
 constexpr int kHotThreads = 1024;     // persistent hot-x CTA: one per SM
+#ifndef GBK_SELL_PIECE
+#define GBK_SELL_PIECE 256
+#endif
+constexpr int kSellPiece = GBK_SELL_PIECE;  // rows longer than this are cut into pieces of this many entries
 constexpr int kMaxHotBytes = 212992;  // shared memory for staged x (208 KiB)
 
 struct SellC {
@@ -67,6 +71,15 @@ struct SellC {
     int64_t ncols = 0;
     int32_t* new_to_old = nullptr;
     void* xr = nullptr;              // renumbered x (ncols)
+    // rows longer than kSellPiece are cut into pieces of kSellPiece entries,
+    // stored as extra rows nreal, nreal + 1, ... whose sums go to `piece`;
+    // k_piece_fold adds each long row's pieces in order
+    int64_t nreal = 0;
+    int64_t npieces = 0;
+    void* piece = nullptr;
+    int64_t nlong = 0;
+    int32_t* long_rows = nullptr;
+    int32_t* long_p0 = nullptr;      // nlong + 1 offsets into piece
 };
 
 struct SegCsr {
@@ -92,6 +105,16 @@ inline unsigned blocks_for(int64_t work, int threads = 256) {
 // ---------------------------------------------------------------------------
 // SELL-C kernels
 
+// Result of stored row r: a real row gets accum(y, acc), a piece of a long
+// row (r >= nreal) parks its sum for k_piece_fold.
+template <typename T>
+__device__ __forceinline__ void sell_store(T* y, T* piece, int64_t nreal, int32_t r, T acc, int accum) {
+    if (r < nreal)
+        y[r] = (accum == GBK_OP_SECOND) ? acc : binop<T>(accum, y[r], acc);
+    else
+        piece[r - nreal] = acc;
+}
+
 // One warp per work item: steps [j0, j0 + kSellChunk) of one slice.  The loop
 // is software-pipelined: the col / val group of the next kSellUnroll steps is
 // loaded before the x values of the current group are gathered, so two
@@ -106,7 +129,7 @@ __global__ void __launch_bounds__(256) k_sell_items(const int32_t* __restrict__ 
                                                     const int32_t* __restrict__ col, const T* __restrict__ val,
                                                     const int32_t* __restrict__ perm, int64_t n, int64_t nitems,
                                                     const T* __restrict__ x, T* __restrict__ y, int accum,
-                                                    T* __restrict__ item_out) {
+                                                    T* __restrict__ item_out, int64_t nreal, T* __restrict__ piece) {
     using S = Semiring<SR, T>;
     constexpr int U = kSellUnroll;
     const int lane = threadIdx.x & 31;
@@ -147,10 +170,7 @@ __global__ void __launch_bounds__(256) k_sell_items(const int32_t* __restrict__ 
     }
     if (slice_item0[s + 1] - slice_item0[s] == 1) {
         const int64_t p = (int64_t)s * kSellC + lane;
-        if (p < n) {
-            const int32_t r = perm[p];
-            y[r] = (accum == GBK_OP_SECOND) ? acc : binop<T>(accum, y[r], acc);
-        }
+        if (p < n) sell_store<T>(y, piece, nreal, perm[p], acc, accum);
     } else {
         item_out[k * kSellC + lane] = acc;
     }
@@ -166,7 +186,7 @@ __global__ void __launch_bounds__(kHotThreads) k_sell_items_hot(
     const int32_t* __restrict__ slice_item0, const int32_t* __restrict__ slice_len,
     const int64_t* __restrict__ slice_ptr, const int32_t* __restrict__ col, const T* __restrict__ val,
     const int32_t* __restrict__ perm, int64_t n, int64_t nitems, int hot, const T* __restrict__ x,
-    T* __restrict__ y, int accum, T* __restrict__ item_out) {
+    T* __restrict__ y, int accum, T* __restrict__ item_out, int64_t nreal, T* __restrict__ piece) {
     using S = Semiring<SR, T>;
     constexpr int U = kSellUnroll;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -215,10 +235,7 @@ __global__ void __launch_bounds__(kHotThreads) k_sell_items_hot(
         }
         if (slice_item0[s + 1] - slice_item0[s] == 1) {
             const int64_t p = (int64_t)s * kSellC + lane;
-            if (p < n) {
-                const int32_t r = perm[p];
-                y[r] = (accum == GBK_OP_SECOND) ? acc : binop<T>(accum, y[r], acc);
-            }
+            if (p < n) sell_store<T>(y, piece, nreal, perm[p], acc, accum);
         } else {
             item_out[k * kSellC + lane] = acc;
         }
@@ -243,7 +260,7 @@ __global__ void k_renumber(int32_t* col, int64_t m, const int32_t* __restrict__ 
 template <int SR, typename T>
 __global__ void k_sell_fold(const int32_t* __restrict__ multi, int64_t nmulti, const int32_t* __restrict__ slice_item0,
                             const T* __restrict__ item_out, const int32_t* __restrict__ perm, int64_t n,
-                            T* __restrict__ y, int accum) {
+                            T* __restrict__ y, int accum, int64_t nreal, T* __restrict__ piece) {
     using S = Semiring<SR, T>;
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t >= nmulti * kSellC) return;
@@ -252,10 +269,7 @@ __global__ void k_sell_fold(const int32_t* __restrict__ multi, int64_t nmulti, c
     T acc = S::identity();
     for (int32_t k = slice_item0[s]; k < slice_item0[s + 1]; k++) acc = S::add(acc, item_out[(int64_t)k * kSellC + lane]);
     const int64_t p = (int64_t)s * kSellC + lane;
-    if (p < n) {
-        const int32_t r = perm[p];
-        y[r] = (accum == GBK_OP_SECOND) ? acc : binop<T>(accum, y[r], acc);
-    }
+    if (p < n) sell_store<T>(y, piece, nreal, perm[p], acc, accum);
 }
 
 // Work items of a slice: ceil(len / kSellChunk), at least 1 (empty slices
@@ -284,31 +298,88 @@ __global__ void k_compact_flags(const int32_t* flag, const int32_t* pos, int64_t
 
 template <typename T>
 __global__ void k_scatter_rows(const int32_t* __restrict__ rows, const T* __restrict__ part, int64_t nr,
-                               T* __restrict__ y, int accum) {
+                               T* __restrict__ y, int accum, int64_t nreal, T* __restrict__ piece) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= nr) return;
-    const int32_t r = rows[k];
-    y[r] = (accum == GBK_OP_SECOND) ? part[k] : binop<T>(accum, y[r], part[k]);
+    sell_store<T>(y, piece, nreal, rows[k], part[k], accum);
+}
+
+// Each long row: its pieces' sums added in piece order, then the accumulator.
+template <int SR, typename T>
+__global__ void k_piece_fold(const int32_t* __restrict__ long_rows, const int32_t* __restrict__ long_p0,
+                             int64_t nlong, const T* __restrict__ piece, T* __restrict__ y, int accum) {
+    using S = Semiring<SR, T>;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nlong) return;
+    T acc = S::identity();
+    for (int32_t k = long_p0[j]; k < long_p0[j + 1]; ++k) acc = S::add(acc, piece[k]);
+    const int32_t r = long_rows[j];
+    y[r] = (accum == GBK_OP_SECOND) ? acc : binop<T>(accum, y[r], acc);
+}
+
+// Virtual rows of the SELL-C build: real rows of at most L entries keep
+// their id; longer rows are replaced by pieces of L entries with ids
+// n + pstart[r] + j.  vlen < 0 marks a replaced real row.
+__global__ void k_piece_counts(const int32_t* __restrict__ ptr, int64_t n, int L, int32_t* np) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r < n) {
+        const int32_t d = ptr[r + 1] - ptr[r];
+        np[r] = d > L ? (d + L - 1) / L : 0;
+    } else if (r == n) {
+        np[n] = 0;
+    }
+}
+
+__global__ void k_virtual_rows(const int32_t* __restrict__ ptr, int64_t n, int L, const int32_t* __restrict__ pstart,
+                               int32_t* vstart, int32_t* vlen, int32_t* keep) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const int32_t b = ptr[r], d = ptr[r + 1] - ptr[r];
+    if (d <= L) {
+        vstart[r] = b;
+        vlen[r] = d;
+        keep[r] = 1;
+        return;
+    }
+    vlen[r] = -1;
+    keep[r] = 0;
+    const int32_t np = (d + L - 1) / L;
+    for (int32_t j = 0; j < np; ++j) {
+        const int64_t id = n + pstart[r] + j;
+        vstart[id] = b + j * L;
+        vlen[id] = min(L, d - j * L);
+        keep[id] = 1;
+    }
+}
+
+__global__ void k_vsigma_keys(const int32_t* __restrict__ vlen, const int32_t* __restrict__ idl, int64_t nv,
+                              int32_t sigma, unsigned long long* keys, int32_t* vals) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    const unsigned long long win = (unsigned long long)(i / sigma);
+    keys[i] = (win << 32) | (unsigned long long)(uint32_t)(0x7fffffff - vlen[idl[i]]);
+    vals[i] = idl[i];
+}
+
+__global__ void k_long_flags(const int32_t* __restrict__ np, int64_t n, int32_t* flag) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r < n) flag[r] = np[r] > 0;
+    else if (r == n) flag[n] = 0;
+}
+
+__global__ void k_long_list(const int32_t* __restrict__ flag, const int32_t* __restrict__ pos,
+                            const int32_t* __restrict__ pstart, int64_t n, int64_t npieces, int32_t* rows,
+                            int32_t* p0) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r < n && flag[r]) {
+        rows[pos[r]] = (int32_t)r;
+        p0[pos[r]] = pstart[r];
+    }
+    if (r == n) p0[pos[n]] = (int32_t)npieces;
 }
 
 // SELL-C build helpers
-__global__ void k_degrees(const int32_t* ptr, int64_t n, int32_t* deg) {
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i < n) deg[i] = ptr[i + 1] - ptr[i];
-}
 
-__global__ void k_sigma_keys(const int32_t* deg, int64_t n, int32_t sigma, unsigned long long* keys, int32_t* ids) {
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    unsigned long long win = (unsigned long long)(i / sigma);
-    keys[i] = (win << 32) | (unsigned long long)(uint32_t)(0x7fffffff - deg[i]);
-    ids[i] = (int32_t)i;
-}
-
-__global__ void k_iota32(int32_t* p, int64_t n) {
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i < n) p[i] = (int32_t)i;
-}
 
 // one warp per slice: longest row and nonzero count; classify overflow
 __global__ void k_slice_stats(const int32_t* deg, const int32_t* perm, int64_t n, int64_t nslices, int32_t* len,
@@ -335,7 +406,8 @@ __global__ void k_slice_stats(const int32_t* deg, const int32_t* perm, int64_t n
 }
 
 template <typename T>
-__global__ void k_sell_fill(const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx, const T* __restrict__ val,
+__global__ void k_sell_fill(const int32_t* __restrict__ vstart, const int32_t* __restrict__ vlen,
+                            const int32_t* __restrict__ idx, const T* __restrict__ val,
                             const int32_t* __restrict__ perm, const int32_t* __restrict__ len,
                             const int64_t* __restrict__ sptr, int64_t n, int32_t* __restrict__ col,
                             T* __restrict__ sval) {
@@ -346,7 +418,7 @@ __global__ void k_sell_fill(const int32_t* __restrict__ ptr, const int32_t* __re
     const int lane = (int)(p % kSellC);
     const int32_t r = perm[p];
     const int64_t base = sptr[s] + lane;
-    for (int32_t e = ptr[r], j = 0; e < ptr[r + 1]; e++, j++) {
+    for (int32_t e = vstart[r], j = 0; j < vlen[r]; e++, j++) {
         col[base + (int64_t)j * kSellC] = idx[e];
         sval[base + (int64_t)j * kSellC] = val[e];
     }
@@ -369,15 +441,15 @@ __global__ void k_ov_compact(const int32_t* flag, const int32_t* pos, const int3
 
 // copy listed rows of a CSR into a compact CSR (warp per row)
 template <typename T>
-__global__ void k_gather_rows(const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                              const T* __restrict__ val, const int32_t* __restrict__ rows,
-                              const int32_t* __restrict__ optr, int64_t nr, int32_t* __restrict__ oidx,
-                              T* __restrict__ oval) {
+__global__ void k_gather_rows(const int32_t* __restrict__ vstart, const int32_t* __restrict__ vlen,
+                              const int32_t* __restrict__ idx, const T* __restrict__ val,
+                              const int32_t* __restrict__ rows, const int32_t* __restrict__ optr, int64_t nr,
+                              int32_t* __restrict__ oidx, T* __restrict__ oval) {
     const int lane = threadIdx.x & 31;
     const int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (k >= nr) return;
     const int32_t r = rows[k];
-    const int32_t b = ptr[r], e = ptr[r + 1], o = optr[k];
+    const int32_t b = vstart[r], e = vstart[r] + vlen[r], o = optr[k];
     for (int32_t q = b + lane; q < e; q += 32) {
         oidx[o + (q - b)] = idx[q];
         oval[o + (q - b)] = val[q];
@@ -506,6 +578,9 @@ int free_sell(SellC* f) {
     cudaFree(f->multi);
     cudaFree(f->new_to_old);
     cudaFree(f->xr);
+    cudaFree(f->piece);
+    cudaFree(f->long_rows);
+    cudaFree(f->long_p0);
     free_view(f->ov);
     delete f;
     return 0;
@@ -595,25 +670,55 @@ int renumber_hot(const CsrView& a, int32_t hot, SellC* f, cudaStream_t s) {
 template <typename T>
 int build_sell(const CsrView& a, int32_t sigma, int32_t hot, int32_t reorder, SellC** out, cudaStream_t s) {
     SellC* f = new SellC();
-    f->n = a.nrows;
     f->sigma = sigma;
     f->ncols = a.ncols;
-    const int64_t n = a.nrows;
-    f->nslices = (n + kSellC - 1) / kSellC;
-    int32_t* deg = nullptr;
-    GBK_CUDA(cudaMalloc(&deg, sizeof(int32_t) * (n > 0 ? n : 1)));
-    GBK_CUDA(cudaMalloc(&f->perm, sizeof(int32_t) * (n > 0 ? n : 1)));
-    if (n > 0) {
-        k_degrees<<<blocks_for(n), 256, 0, s>>>(a.ptr, n, deg);
+    const int64_t nr = a.nrows;
+    f->nreal = nr;
+    // virtual rows: rows of at most kSellPiece entries, and kSellPiece-entry
+    // pieces of the longer ones (ids nr, nr + 1, ...)
+    int32_t *np = nullptr, *pstart = nullptr;
+    GBK_CUDA(cudaMalloc(&np, sizeof(int32_t) * (nr + 1)));
+    GBK_CUDA(cudaMalloc(&pstart, sizeof(int32_t) * (nr + 1)));
+    k_piece_counts<<<blocks_for(nr + 1), 256, 0, s>>>(a.ptr, nr, kSellPiece, np);
+    GBK_LAUNCHED();
+    int rc0 = cub_scan_excl(np, pstart, nr + 1, s);
+    if (rc0) return rc0;
+    int32_t npieces = 0;
+    GBK_CUDA(cudaMemcpyAsync(&npieces, pstart + nr, 4, cudaMemcpyDeviceToHost, s));
+    GBK_CUDA(cudaStreamSynchronize(s));
+    f->npieces = npieces;
+    const int64_t nvt = nr + npieces;
+    int32_t *vstart = nullptr, *deg = nullptr, *keep = nullptr, *kpos = nullptr, *idl = nullptr;
+    GBK_CUDA(cudaMalloc(&vstart, sizeof(int32_t) * (nvt > 0 ? nvt : 1)));
+    GBK_CUDA(cudaMalloc(&deg, sizeof(int32_t) * (nvt > 0 ? nvt : 1)));  // vlen, indexed by virtual id
+    GBK_CUDA(cudaMalloc(&keep, sizeof(int32_t) * (nvt + 1)));
+    GBK_CUDA(cudaMalloc(&kpos, sizeof(int32_t) * (nvt + 1)));
+    GBK_CUDA(cudaMemsetAsync(keep + nvt, 0, sizeof(int32_t), s));
+    if (nr > 0) {
+        k_virtual_rows<<<blocks_for(nr), 256, 0, s>>>(a.ptr, nr, kSellPiece, pstart, vstart, deg, keep);
         GBK_LAUNCHED();
     }
+    rc0 = cub_scan_excl(keep, kpos, nvt + 1, s);
+    if (rc0) return rc0;
+    int32_t nv32 = 0;
+    GBK_CUDA(cudaMemcpyAsync(&nv32, kpos + nvt, 4, cudaMemcpyDeviceToHost, s));
+    GBK_CUDA(cudaStreamSynchronize(s));
+    const int64_t n = nv32;
+    f->n = n;
+    f->nslices = (n + kSellC - 1) / kSellC;
+    GBK_CUDA(cudaMalloc(&idl, sizeof(int32_t) * (n > 0 ? n : 1)));
+    if (nvt > 0) {
+        k_compact_flags<<<blocks_for(nvt), 256, 0, s>>>(keep, kpos, nvt, idl);
+        GBK_LAUNCHED();
+    }
+    GBK_CUDA(cudaMalloc(&f->perm, sizeof(int32_t) * (n > 0 ? n : 1)));
     if (sigma > 1 && n > 1) {
         unsigned long long *keys = nullptr, *keys2 = nullptr;
         int32_t* ids = nullptr;
         GBK_CUDA(cudaMalloc(&keys, sizeof(unsigned long long) * n));
         GBK_CUDA(cudaMalloc(&keys2, sizeof(unsigned long long) * n));
         GBK_CUDA(cudaMalloc(&ids, sizeof(int32_t) * n));
-        k_sigma_keys<<<blocks_for(n), 256, 0, s>>>(deg, n, sigma, keys, ids);
+        k_vsigma_keys<<<blocks_for(n), 256, 0, s>>>(deg, idl, n, sigma, keys, ids);
         GBK_LAUNCHED();
         size_t tb = 0;
         cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, ids, f->perm, (int)n, 0, 64, s);
@@ -627,8 +732,29 @@ int build_sell(const CsrView& a, int32_t sigma, int32_t hot, int32_t reorder, Se
         cudaFree(keys2);
         cudaFree(ids);
     } else if (n > 0) {
-        k_iota32<<<blocks_for(n), 256, 0, s>>>(f->perm, n);
+        GBK_CUDA(cudaMemcpyAsync(f->perm, idl, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
+    }
+    // long rows and their piece ranges, for k_piece_fold
+    if (npieces > 0) {
+        int32_t *lflag = nullptr, *lpos = nullptr;
+        GBK_CUDA(cudaMalloc(&lflag, sizeof(int32_t) * (nr + 1)));
+        GBK_CUDA(cudaMalloc(&lpos, sizeof(int32_t) * (nr + 1)));
+        k_long_flags<<<blocks_for(nr + 1), 256, 0, s>>>(np, nr, lflag);
         GBK_LAUNCHED();
+        rc0 = cub_scan_excl(lflag, lpos, nr + 1, s);
+        if (rc0) return rc0;
+        int32_t nl = 0;
+        GBK_CUDA(cudaMemcpyAsync(&nl, lpos + nr, 4, cudaMemcpyDeviceToHost, s));
+        GBK_CUDA(cudaStreamSynchronize(s));
+        f->nlong = nl;
+        GBK_CUDA(cudaMalloc(&f->long_rows, sizeof(int32_t) * (nl > 0 ? nl : 1)));
+        GBK_CUDA(cudaMalloc(&f->long_p0, sizeof(int32_t) * (nl + 1)));
+        k_long_list<<<blocks_for(nr + 1), 256, 0, s>>>(lflag, lpos, pstart, nr, npieces, f->long_rows, f->long_p0);
+        GBK_LAUNCHED();
+        GBK_CUDA(cudaMalloc(&f->piece, sizeof(T) * npieces));
+        GBK_CUDA(cudaStreamSynchronize(s));
+        cudaFree(lflag);
+        cudaFree(lpos);
     }
     const int64_t ns = f->nslices;
     int32_t* is_ov = nullptr;
@@ -658,7 +784,7 @@ int build_sell(const CsrView& a, int32_t sigma, int32_t hot, int32_t reorder, Se
     GBK_CUDA(cudaMemsetAsync(f->col, 0xff, sizeof(int32_t) * (f->padded > 0 ? f->padded : 1), s));
     GBK_CUDA(cudaMemsetAsync(f->val, 0, sizeof(T) * (f->padded > 0 ? f->padded : 1), s));
     if (n > 0) {
-        k_sell_fill<T><<<blocks_for(n), 256, 0, s>>>(a.ptr, a.idx, (const T*)a.val, f->perm, f->slice_len,
+        k_sell_fill<T><<<blocks_for(n), 256, 0, s>>>(vstart, deg, a.idx, (const T*)a.val, f->perm, f->slice_len,
                                                       f->slice_ptr, n, f->col, (T*)f->val);
         GBK_LAUNCHED();
     }
@@ -731,8 +857,8 @@ int build_sell(const CsrView& a, int32_t sigma, int32_t hot, int32_t reorder, Se
             o.nnz = onnz;
             GBK_CUDA(cudaMalloc(&o.idx, sizeof(int32_t) * (onnz > 0 ? onnz : 1)));
             GBK_CUDA(cudaMalloc(&o.val, sizeof(T) * (onnz > 0 ? onnz : 1)));
-            k_gather_rows<T><<<blocks_for(nov * 32), 256, 0, s>>>(a.ptr, a.idx, (const T*)a.val, f->ov_rows, o.ptr,
-                                                                   nov, o.idx, (T*)o.val);
+            k_gather_rows<T><<<blocks_for(nov * 32), 256, 0, s>>>(vstart, deg, a.idx, (const T*)a.val, f->ov_rows,
+                                                                   o.ptr, nov, o.idx, (T*)o.val);
             GBK_LAUNCHED();
             rc = build_tiles(o, sizeof(T), s);
             if (rc) return rc;
@@ -746,6 +872,12 @@ int build_sell(const CsrView& a, int32_t sigma, int32_t hot, int32_t reorder, Se
     cudaFree(is_ov);
     cudaFree(stored);
     cudaFree(deg);
+    cudaFree(vstart);
+    cudaFree(np);
+    cudaFree(pstart);
+    cudaFree(keep);
+    cudaFree(kpos);
+    cudaFree(idl);
     if ((hot > 0 || reorder) && a.ncols > 0) {
         int rc = renumber_hot(a, hot, f, s);
         if (rc) return rc;
@@ -949,24 +1081,31 @@ int run_sell(const SellC* f, int accum, const T* x, T* y, cudaStream_t s) {
         if (f->nitems > 0) {
             k_sell_items_hot<SR, T><<<(unsigned)num_sms(), kHotThreads, smem, s>>>(
                 f->item_slice, f->item_j0, f->slice_item0, f->slice_len, f->slice_ptr, f->col, (const T*)f->val,
-                f->perm, f->n, f->nitems, f->hot, x, y, accum, (T*)f->item_out);
+                f->perm, f->n, f->nitems, f->hot, x, y, accum, (T*)f->item_out, f->nreal, (T*)f->piece);
             GBK_LAUNCHED();
         }
     } else if (f->nitems > 0) {
         k_sell_items<SR, T><<<blocks_for(f->nitems * 32), 256, 0, s>>>(
             f->item_slice, f->item_j0, f->slice_item0, f->slice_len, f->slice_ptr, f->col, (const T*)f->val, f->perm,
-            f->n, f->nitems, x, y, accum, (T*)f->item_out);
+            f->n, f->nitems, x, y, accum, (T*)f->item_out, f->nreal, (T*)f->piece);
         GBK_LAUNCHED();
     }
     if (f->nmulti > 0) {
         k_sell_fold<SR, T><<<blocks_for(f->nmulti * kSellC), 256, 0, s>>>(
-            f->multi, f->nmulti, f->slice_item0, (const T*)f->item_out, f->perm, f->n, y, accum);
+            f->multi, f->nmulti, f->slice_item0, (const T*)f->item_out, f->perm, f->n, y, accum, f->nreal,
+            (T*)f->piece);
         GBK_LAUNCHED();
     }
     if (f->nov > 0) {
         int rc = spmv_csr(f->ov, SR, GBK_OP_SECOND, dtype_of_t<T>(), x, f->ov_out, nullptr, 0, 0, s);
         if (rc) return rc;
-        k_scatter_rows<T><<<blocks_for(f->nov), 256, 0, s>>>(f->ov_rows, (const T*)f->ov_out, f->nov, y, accum);
+        k_scatter_rows<T><<<blocks_for(f->nov), 256, 0, s>>>(f->ov_rows, (const T*)f->ov_out, f->nov, y, accum,
+                                                             f->nreal, (T*)f->piece);
+        GBK_LAUNCHED();
+    }
+    if (f->nlong > 0) {
+        k_piece_fold<SR, T><<<blocks_for(f->nlong), 256, 0, s>>>(f->long_rows, f->long_p0, f->nlong,
+                                                                 (const T*)f->piece, y, accum);
         GBK_LAUNCHED();
     }
     return GBK_SUCCESS;
