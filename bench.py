@@ -238,8 +238,11 @@ def dominant_kernel(fmt_name, scale, graph):
     """(kernel description, profile summary) for the storage format that ran."""
     tag = f"{graph}{scale}"
     if fmt_name == "SELL_C":
-        return ("k_sell_items (+ k_sell_fold; rows of problematic slices through k_spmv_binned); achieved counts "
-                "the whole SpMV", f"spmv_sell_c_{tag}")
+        return ("k_sell_items (+ k_piece_fold for long-row pieces, k_sell_fold, k_spmv_binned for the few "
+                "problematic slices); achieved counts the whole SpMV", f"spmv_sell_c_{tag}")
+    if fmt_name == "CSR_SEG":
+        return "k_segsmem (x windows staged in shared memory); achieved counts the whole SpMV", \
+            f"spmv_csr_seg_staged_{tag}"
     if fmt_name == "CSR":
         return "k_spmv_binned (+ k_spmv_split_fixup); achieved counts the whole SpMV", f"spmv_csr_kernels_{tag}"
     return f"{fmt_name} kernels; achieved counts the whole SpMV", f"spmv_{fmt_name.lower()}_{tag}"
