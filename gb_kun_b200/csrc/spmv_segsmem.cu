@@ -6,13 +6,20 @@
 // merges them.  Here a window is kSegCols columns, the size of x that fits a
 // CTA's shared memory (192 KiB of 4-byte values):
 //   * the entries are re-sorted segment-major (then by row, then column), each
-//     with a 16-bit column inside its window; a bit per entry marks the start
-//     of a "virtual row" (the entries of one row inside one segment);
-//   * 148 persistent CTAs (one per SM, 1024 threads) take equal shares of the
-//     entries; for each segment it touches a CTA copies that window of x into
-//     shared memory once, and its warps walk 32-entry chunks of their share:
-//     coalesced 2-byte column / 4-byte value loads, the x gather from shared
-//     memory, a segmented warp scan along the row-start bits;
+//     with a 16-bit column inside its window; the entries of one row inside
+//     one segment form a "virtual row";
+//   * the entries are cut into 256-entry chunks; lane l of a warp owns entries
+//     8 l .. 8 l + 7 of a chunk, and a 16-bit group record per 8 entries holds
+//     their virtual-row start bits and the number of starts earlier in the
+//     chunk, so a lane knows its virtual rows without a scan;
+//   * 148 persistent CTAs (one per SM, 768 threads) take shares of whole
+//     chunks of equal estimated cost (entries, virtual rows and windows, each
+//     weighted by its measured cost); for each segment it touches a CTA copies
+//     that window of x into shared memory once (16-byte asynchronous copies),
+//     and its warps walk whole chunks: 16-byte column / value loads one chunk
+//     ahead, eight gathers from shared memory per lane, a sequential
+//     segmented sum per lane and ONE segmented warp scan per 256 entries for
+//     the virtual row that crosses lanes;
 //   * each virtual row's sum goes straight into y with one atomic of the
 //     semiring's add (float / int add, int / float minimum, or a store of 1
 //     for the logical-or semirings), so there is no merge pass.
@@ -22,6 +29,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "common.cuh"
@@ -30,20 +38,25 @@
 namespace gbk {
 
 constexpr int kSegCols = 49152;  // x values per staged window (192 KiB of 4-byte values)
-constexpr int kSegThreads = 1024;
-constexpr int kSegUnroll = 4;    // 32-entry chunks whose loads a warp keeps in flight
+constexpr int kSegThreads = 768;
+constexpr int kLaneEntries = 8;                  // entries per lane of a chunk
+constexpr int kChunk = 32 * kLaneEntries;        // entries per warp chunk
+constexpr int kGroups = kChunk / kLaneEntries;   // group records per chunk (one per lane)
 
 struct SegSmem {
     int64_t nrows = 0, ncols = 0, nnz = 0, nvrows = 0;
+    int64_t nchunks = 0;
     int32_t nseg = 0;
-    uint16_t* col = nullptr;       // column inside the window, nnz
-    void* val = nullptr;           // nnz
-    uint32_t* head = nullptr;      // one bit per entry: starts a virtual row (nnz padded to 32)
-    int32_t* chunk_vr = nullptr;   // virtual row containing entry 32 k
+    uint16_t* col = nullptr;       // column inside the window, nchunks * kChunk (zero padded)
+    void* val = nullptr;           // nchunks * kChunk (zero padded)
+    uint16_t* grp = nullptr;       // per 8 entries: (virtual-row starts earlier in the chunk) << 8 | start bits
+    int32_t* cvr = nullptr;        // nchunks + 1: virtual row open just before entry kChunk * q (-1 at 0)
     int32_t* vrow = nullptr;       // original row of each virtual row
     int32_t* seg_start = nullptr;  // nseg + 1 entry offsets
+    int32_t nshares = 0;           // CTAs of the SpMV launch (one per SM)
+    int32_t* share = nullptr;      // nshares + 1 entry offsets of the CTAs' shares (chunk aligned)
     void* tmp = nullptr;           // nrows: the product before the accumulator
-    int32_t* err = nullptr;        // first out-of-range index seen by the kernel (0 = none)
+    int32_t* err = nullptr;        // first failed index check seen by the kernel (0 = none)
     bool check = true;             // read err back after the first launch
 };
 
@@ -61,38 +74,46 @@ __global__ void k_ss_keys(const int32_t* __restrict__ ptr, const int32_t* __rest
 
 template <typename T>
 __global__ void k_ss_fill(const unsigned long long* __restrict__ keys, const int32_t* __restrict__ pos,
-                          const int32_t* __restrict__ idx, const T* __restrict__ v, int64_t nnz, int64_t padded,
+                          const int32_t* __restrict__ idx, const T* __restrict__ v, int64_t nnz,
                           uint16_t* __restrict__ col, T* __restrict__ val, int32_t* __restrict__ flag,
-                          uint32_t* __restrict__ head, int32_t* __restrict__ seg_start) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;  // padded is a multiple of 32
-    if (i >= padded) return;
-    bool h = false;
-    if (i < nnz) {
-        const unsigned long long k = keys[i];
-        const int32_t seg = (int32_t)(k >> 32);
-        const int32_t e = pos[i];
-        col[i] = (uint16_t)(idx[e] - seg * kSegCols);
-        val[i] = v[e];
-        h = (i == 0) || (keys[i - 1] != k);
-        flag[i] = h;
-        if (i == 0 || (int32_t)(keys[i - 1] >> 32) != seg) seg_start[seg] = (int32_t)i;
-    }
-    const unsigned w = __ballot_sync(0xffffffffu, h);
-    if ((threadIdx.x & 31) == 0) head[i >> 5] = w;
+                          int32_t* __restrict__ seg_start) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnz) return;
+    const unsigned long long k = keys[i];
+    const int32_t seg = (int32_t)(k >> 32);
+    const int32_t e = pos[i];
+    col[i] = (uint16_t)(idx[e] - seg * kSegCols);
+    val[i] = v[e];
+    flag[i] = (i == 0) || (keys[i - 1] != k);
+    if (i == 0 || (int32_t)(keys[i - 1] >> 32) != seg) seg_start[seg] = (int32_t)i;
 }
 
 __global__ void k_ss_vrows(const unsigned long long* __restrict__ keys, const int32_t* __restrict__ flag,
-                           const int32_t* __restrict__ vid, int64_t nnz, int32_t* __restrict__ vrow,
-                           int32_t* __restrict__ chunk_vr) {
+                           const int32_t* __restrict__ vid, int64_t nnz, int32_t* __restrict__ vrow) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nnz) return;
     if (flag[i]) vrow[vid[i]] = (int32_t)(keys[i] & 0xffffffffu);
-    if ((i & 31) == 0) chunk_vr[i >> 5] = vid[i] + flag[i] - 1;
 }
 
-// atomic fold of one virtual row's sum into out[r] by the semiring's add
-template <int SR, typename T>
-__device__ __forceinline__ void fold_into(T* out, int32_t r, T v);
+// Group records and chunk starts from the start flags and their exclusive
+// scan vid (vid[i] = virtual rows starting before entry i, vid[nnz] = total).
+__global__ void k_ss_groups(const int32_t* __restrict__ flag, const int32_t* __restrict__ vid, int64_t nnz,
+                            int64_t ngroups, uint16_t* __restrict__ grp) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ngroups) return;
+    const int64_t e0 = g * kLaneEntries, cb = (g / kGroups) * kChunk;
+    unsigned bits = 0;
+    for (int i = 0; i < kLaneEntries; ++i)
+        if (e0 + i < nnz && flag[e0 + i]) bits |= 1u << i;
+    const int32_t before = vid[min(e0, nnz)] - vid[min(cb, nnz)];  // < kChunk
+    grp[g] = (uint16_t)(((unsigned)before << 8) | bits);
+}
+
+__global__ void k_ss_cvr(const int32_t* __restrict__ vid, int64_t nnz, int64_t nchunks, int32_t* __restrict__ cvr) {
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q > nchunks) return;
+    cvr[q] = vid[min(q * kChunk, nnz)] - 1;
+}
 
 __device__ __forceinline__ void atomic_min_any(float* p, float v) {
     // order-preserving on the bit patterns: non-negative floats order as ints,
@@ -124,129 +145,187 @@ struct AddClass {  // 0 plus, 1 min, 2 or, -1 not folded atomically
                                                                                       : -1;
 };
 
+// Does folding v into y change anything?  (The identity of the add never
+// does, so empty and masked-out runs cost no atomic.)
 template <int SR, typename T>
-__device__ __forceinline__ void fold_into(T* out, int32_t r, T v) {
+__device__ __forceinline__ bool changes(T v) {
     using S = Semiring<SR, T>;
     constexpr int cls = AddClass<SR>::value;
-    if constexpr (cls == 0) {
-        if (v != T(0)) atomic_add_any(out + r, v);
-    } else if constexpr (cls == 1) {
-        if (v < S::identity()) atomic_min_any(out + r, v);
-    } else {
-        if (v != T(0)) out[r] = T(1);
-    }
+    if constexpr (cls == 1)
+        return v < S::identity();
+    else
+        return v != T(0);
 }
 
-// One warp over entries [wa, wb) of the staged segment.
+// atomic fold of one virtual row's sum into out[r] by the semiring's add
+template <int SR, typename T>
+__device__ __forceinline__ void fold_into(T* out, int32_t r, T v) {
+    constexpr int cls = AddClass<SR>::value;
+    if constexpr (cls == 0)
+        atomic_add_any(out + r, v);
+    else if constexpr (cls == 1)
+        atomic_min_any(out + r, v);
+    else
+        out[r] = T(1);
+}
+
 // Index checks: a virtual row, row or window column out of range is recorded
-// in *err (first one wins) and the access skipped, so a malformed structure
-// reports an error instead of touching memory it does not own.
+// in *err (first one wins) and the access skipped or clamped, so a malformed
+// structure reports an error instead of touching memory it does not own.
 __device__ __forceinline__ void ss_flag(int32_t* err, int32_t code) { atomicCAS(err, 0, code); }
 
 template <int SR, typename T>
-__device__ __forceinline__ void ss_warp_range(const uint16_t* __restrict__ col, const T* __restrict__ val,
-                                              const uint32_t* __restrict__ head,
-                                              const int32_t* __restrict__ chunk_vr,
-                                              const int32_t* __restrict__ vrow, const T* xs, int w, int64_t wa,
-                                              int64_t wb, T* out, int64_t nvrows, int64_t nrows,
-                                              int32_t* err) {
+__device__ __forceinline__ void ss_emit(T* out, int32_t r, T v, int64_t nrows, int32_t* err) {
+    if (!changes<SR, T>(v)) return;
+    if (r < 0 || r >= nrows)
+        ss_flag(err, 2);
+    else
+        fold_into<SR, T>(out, r, v);
+}
+
+template <typename T> __device__ __forceinline__ T from_bits(uint32_t u);
+template <> __device__ __forceinline__ float from_bits<float>(uint32_t u) { return __uint_as_float(u); }
+template <> __device__ __forceinline__ int32_t from_bits<int32_t>(uint32_t u) { return (int32_t)u; }
+
+// One warp over chunks [q0, q1) of the staged segment, restricted to the
+// entries [a, b) (the first and last chunk may hold entries of a neighbouring
+// segment or of another CTA's share: those add the identity, but their
+// virtual-row starts still count, so the row numbering stays global).
+template <int SR, typename T>
+__device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, const uint4* __restrict__ val4,
+                                               const uint16_t* __restrict__ grp, const int32_t* __restrict__ cvr,
+                                               const int32_t* __restrict__ vrow, const T* xs, int w, int64_t q0,
+                                               int64_t q1, int64_t a, int64_t b, T* out, int64_t nvrows,
+                                               int64_t nrows, int32_t* err) {
     using S = Semiring<SR, T>;
     const unsigned kAll = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned le = (lane == 31) ? kAll : ((2u << lane) - 1u);
-    // the virtual row open just before entry wa
-    const int64_t k = wa >> 5;
-    const int b = (int)(wa & 31);
-    const uint32_t hw = head[k];
-    const int32_t vr_at_wa = chunk_vr[k] + __popc(hw & (b == 31 ? 0xfffffffeu : (((2u << b) - 1u) & ~1u)));
-    int64_t vr_open = ((hw >> b) & 1) ? (int64_t)vr_at_wa - 1 : (int64_t)vr_at_wa;
-    T carry = S::identity();
-    for (int64_t e0 = wa; e0 < wb; e0 += 32 * kSegUnroll) {
-        uint16_t cc[kSegUnroll];
-        T vv[kSegUnroll];
-        unsigned H[kSegUnroll];
-#pragma unroll
-        for (int u = 0; u < kSegUnroll; ++u) {
-            const int64_t e = e0 + u * 32 + lane;
-            const bool ok = e < wb;
-            cc[u] = ok ? __ldcs(col + e) : (uint16_t)0;
-            vv[u] = ok ? __ldcs(val + e) : T(0);
-            const uint32_t hw = ok ? __ldg(head + (e >> 5)) : 0u;
-            H[u] = __ballot_sync(kAll, ok && ((hw >> (e & 31)) & 1u));
+    const unsigned wl = (unsigned)(w - 1);  // last column of the window
+    const unsigned wl2 = wl | (wl << 16);
+    T carry = S::identity();  // the virtual row open at the end of the previous chunk
+    uint4 cn = __ldcs(col8 + q0 * kGroups + lane);
+    uint4 an = __ldcs(val4 + q0 * 2 * kGroups + 2 * lane);
+    uint4 bn = __ldcs(val4 + q0 * 2 * kGroups + 2 * lane + 1);
+    uint32_t gn = __ldcs(grp + q0 * kGroups + lane);
+    int32_t vn = __ldg(cvr + q0);
+    for (int64_t q = q0; q < q1; ++q) {
+        const uint4 c = cn, va = an, vb = bn;
+        const uint32_t g = gn;
+        const int32_t cv = vn;
+        if (q + 1 < q1) {  // the next chunk's loads go out before this chunk's work
+            cn = __ldcs(col8 + (q + 1) * kGroups + lane);
+            an = __ldcs(val4 + (q + 1) * 2 * kGroups + 2 * lane);
+            bn = __ldcs(val4 + (q + 1) * 2 * kGroups + 2 * lane + 1);
+            gn = __ldcs(grp + (q + 1) * kGroups + lane);
+            vn = __ldg(cvr + q + 1);
         }
-        // does the entry after this group start a virtual row?
-        const int64_t en = e0 + 32 * kSegUnroll;
-        const bool next_group_head = en < wb && ((__ldg(head + (en >> 5)) >> (en & 31)) & 1u);
-        // the virtual rows these chunks touch are consecutive: fetch their row
-        // ids together (lane j of chunk u holds virtual row vb[u] + off[u] + j)
-        int32_t rr[kSegUnroll];
-        int64_t vb[kSegUnroll];
-        int off[kSegUnroll];
-        {
-            int64_t base = vr_open;
+        const uint32_t hb = g & 0xffu;                    // entries of this lane that start a virtual row
+        const int32_t vr_lane = cv + (int32_t)(g >> 8);   // virtual row open before this lane's entries
+        // rows of the virtual rows that end at this lane's starts (the i-th
+        // start closes virtual row vr_lane + number of starts before it)
+        int32_t r[kLaneEntries];
 #pragma unroll
-            for (int u = 0; u < kSegUnroll; ++u) {
-                vb[u] = base;
-                off[u] = (int)(H[u] & 1u);
-                const int64_t q = base + off[u] + lane;
-                rr[u] = (q >= 0 && q < nvrows) ? __ldg(vrow + q) : -1;
-                base += __popc(H[u]);
+        for (int i = 0; i < kLaneEntries; ++i) {
+            r[i] = -1;
+            if ((hb >> i) & 1u) {
+                const int64_t vr = (int64_t)vr_lane + __popc(hb & ((1u << i) - 1u));
+                if (vr >= 0 && vr < nvrows) r[i] = __ldg(vrow + vr);
             }
         }
+        // a ragged chunk: entries outside [a, b) (another window's columns, or
+        // another share) read column 0 and add the identity
+        const int64_t cb = q * kChunk, e0 = cb + lane * kLaneEntries;
+        const bool ragged = cb < a || cb + kChunk > b;
+        uint32_t cr[4] = {c.x, c.y, c.z, c.w};
+        if (ragged) {
 #pragma unroll
-        for (int u = 0; u < kSegUnroll; ++u) {
-            const int64_t eb = e0 + u * 32;
-            if (eb >= wb) break;
-            const int64_t e = eb + lane;
-            const bool ok = e < wb;
-            const bool in_win = cc[u] < w;
-            if (ok && !in_win) ss_flag(err, 1);
-            T v = (ok && in_win) ? S::mul(vv[u], xs[cc[u]]) : S::identity();
-            const unsigned hle = H[u] & le;
-            const int first = hle ? 31 - __clz(hle) : 0;  // first lane of this lane's run in the chunk
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const T o = __shfl_up_sync(kAll, v, d);
-                if (lane - d >= first) v = S::add(v, o);
-            }
-            if (!hle) v = S::add(carry, v);  // the run continues the open virtual row
-            const int j = __popc(hle);       // this run is virtual row vb[u] + j
-            const int32_t r = __shfl_sync(kAll, rr[u], (j - off[u]) & 31);
-            const int last = (int)min((int64_t)31, wb - 1 - eb);  // last valid lane of the chunk
-            const bool next_head = lane < 31 && ((H[u] >> (lane + 1)) & 1u);
-            // the run at `last` goes on into the next entry unless that starts a row
-            bool cont = false;
-            if (e + 1 < wb || eb + 32 < wb) {
-                const bool nh = (u + 1 < kSegUnroll) ? (bool)(H[(u + 1) % kSegUnroll] & 1u) : next_group_head;
-                cont = (last == 31) && (eb + 32 < wb) && !nh;
-            }
-            cont = __shfl_sync(kAll, cont, last);
-            if (ok && (next_head || (lane == last && !cont))) {
-                const int64_t vr = vb[u] + j;
-                if (vr < 0 || vr >= nvrows || r < 0 || r >= nrows)
-                    ss_flag(err, 2);
-                else
-                    fold_into<SR, T>(out, r, v);
-            }
-            carry = cont ? __shfl_sync(kAll, v, last) : S::identity();
+            for (int i = 0; i < kLaneEntries; ++i)
+                if (e0 + i < a || e0 + i >= b) cr[i >> 1] &= (i & 1) ? 0x0000ffffu : 0xffff0000u;
         }
-        {
+        // products; columns are clamped into the window and a column outside
+        // it is reported
+        const uint32_t cmax = __vmaxu2(__vmaxu2(cr[0], cr[1]), __vmaxu2(cr[2], cr[3]));
+        if ((cmax & 0xffffu) > wl || (cmax >> 16) > wl) ss_flag(err, 1);
+        const uint32_t vw[kLaneEntries] = {va.x, va.y, va.z, va.w, vb.x, vb.y, vb.z, vb.w};
+        T p[kLaneEntries];
 #pragma unroll
-            for (int u = 0; u < kSegUnroll; ++u) vr_open += __popc(H[u]);
+        for (int i = 0; i < kLaneEntries; ++i) {
+            const uint32_t cw = __vminu2(cr[i >> 1], wl2);
+            const uint32_t ci = (i & 1) ? (cw >> 16) : (cw & 0xffffu);
+            p[i] = S::mul(from_bits<T>(vw[i]), xs[ci]);
         }
+        if (ragged) {
+#pragma unroll
+            for (int i = 0; i < kLaneEntries; ++i)
+                if (e0 + i < a || e0 + i >= b) p[i] = S::identity();
+        }
+        // sequential segmented sum: em[i] is the run closed by a start at i
+        T em[kLaneEntries];
+        T acc = S::identity();
+#pragma unroll
+        for (int i = 0; i < kLaneEntries; ++i) {
+            em[i] = acc;
+            acc = ((hb >> i) & 1u) ? p[i] : S::add(acc, p[i]);
+        }
+        // segmented warp scan of the lane tails: s = the run open after this
+        // lane, including earlier lanes (and the previous chunk's carry) when
+        // no start lies between
+        const unsigned hle = __ballot_sync(kAll, hb != 0) & le;
+        const int first = hle ? 31 - __clz(hle) : 0;  // last lane at or before this one with a start
+        T s = acc;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const T o = __shfl_up_sync(kAll, s, d);
+            if (lane - d >= first) s = S::add(s, o);
+        }
+        if (!hle) s = S::add(carry, s);
+        T xin = __shfl_up_sync(kAll, s, 1);  // the run open before this lane
+        if (lane == 0) xin = carry;
+        carry = __shfl_sync(kAll, s, 31);
+        // fold the closed runs; the first start closes the run that came in
+        const int f = __ffs(hb) - 1;
+#pragma unroll
+        for (int i = 0; i < kLaneEntries; ++i)
+            if ((hb >> i) & 1u) ss_emit<SR, T>(out, r[i], i == f ? S::add(xin, em[i]) : em[i], nrows, err);
     }
+    // the run still open after the last chunk
+    if (lane == 0 && changes<SR, T>(carry)) {
+        const int32_t vr = __ldg(cvr + q1);
+        ss_emit<SR, T>(out, (vr >= 0 && vr < nvrows) ? __ldg(vrow + vr) : -1, carry, nrows, err);
+    }
+}
+
+// Copy w values of x into the shared window with 16-byte asynchronous copies
+// (all of a thread's copies in flight at once, no registers held), scalar
+// loads for a misaligned source and the last w % 4 values.  Returns once this
+// thread's copies have landed; the caller's barrier publishes them.
+template <typename T>
+__device__ __forceinline__ void stage_window(T* xs, const T* src, int w) {
+    int done = 0;
+    if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+        const int n16 = w >> 2;
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(xs);
+        for (int i = threadIdx.x; i < n16; i += blockDim.x)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 16u * (uint32_t)i), "l"(src + 4 * i)
+                         : "memory");
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        done = n16 * 4;
+    }
+    for (int i = done + threadIdx.x; i < w; i += blockDim.x) xs[i] = __ldg(src + i);
+    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 template <int SR, typename T>
 __global__ void __launch_bounds__(kSegThreads, 1)
-    k_segsmem(const uint16_t* __restrict__ col, const T* __restrict__ val, const uint32_t* __restrict__ head,
-              const int32_t* __restrict__ chunk_vr, const int32_t* __restrict__ vrow,
-              const int32_t* __restrict__ seg_start, int32_t nseg, int64_t nnz, int64_t ncols, int64_t nvrows,
-              int64_t nrows, const T* __restrict__ x, T* out, int32_t* err) {
+    k_segsmem(const uint16_t* __restrict__ col, const T* __restrict__ val, const uint16_t* __restrict__ grp,
+              const int32_t* __restrict__ cvr, const int32_t* __restrict__ vrow,
+              const int32_t* __restrict__ seg_start, const int32_t* __restrict__ share, int32_t nseg,
+              int64_t ncols, int64_t nvrows, int64_t nrows, const T* __restrict__ x, T* out, int32_t* err) {
     extern __shared__ __align__(16) unsigned char ss_smem[];
     T* xs = reinterpret_cast<T*>(ss_smem);
     const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const int64_t c0 = nnz * blockIdx.x / gridDim.x, c1 = nnz * (blockIdx.x + 1) / gridDim.x;
+    const int64_t c0 = share[blockIdx.x], c1 = share[blockIdx.x + 1];
     if (c0 >= c1) return;  // the whole block leaves together
     int lo = 0, hi = nseg;  // last segment starting at or before c0
     while (hi - lo > 1) {
@@ -256,19 +335,21 @@ __global__ void __launch_bounds__(kSegThreads, 1)
         else
             hi = mid;
     }
+    const uint4* col8 = reinterpret_cast<const uint4*>(col);
+    const uint4* val4 = reinterpret_cast<const uint4*>(val);
     for (int s = lo; s < nseg && seg_start[s] < c1; ++s) {
         const int64_t a = max(c0, (int64_t)seg_start[s]), b = min(c1, (int64_t)seg_start[s + 1]);
         if (a >= b) continue;
         __syncthreads();  // the previous window's readers are done
         const int64_t col0 = (int64_t)s * kSegCols;
         const int w = (int)min((int64_t)kSegCols, ncols - col0);
-        for (int i = threadIdx.x; i < w; i += blockDim.x) xs[i] = __ldg(x + col0 + i);
+        stage_window(xs, x + col0, w);
         __syncthreads();
-        const int64_t nch = (b - a + 31) >> 5;
-        const int64_t per = (nch + nwarps - 1) / nwarps;
-        const int64_t wa = a + (int64_t)warp * per * 32;
-        const int64_t wb = min(b, wa + per * 32);
-        if (wa < wb) ss_warp_range<SR, T>(col, val, head, chunk_vr, vrow, xs, w, wa, wb, out, nvrows, nrows, err);
+        const int64_t qa = a / kChunk, qb = (b + kChunk - 1) / kChunk;
+        const int64_t per = (qb - qa + nwarps - 1) / nwarps;
+        const int64_t q0 = qa + (int64_t)warp * per, q1 = min(qb, q0 + per);
+        if (q0 < q1)
+            ss_warp_chunks<SR, T>(col8, val4, grp, cvr, vrow, xs, w, q0, q1, a, b, out, nvrows, nrows, err);
     }
 }
 
@@ -286,6 +367,45 @@ __global__ void k_ss_accum(T* __restrict__ y, const T* __restrict__ t, int64_t n
 
 unsigned blocks(int64_t n) { return (unsigned)((n + 255) / 256); }
 
+// Relative costs of the work a CTA does, in entries: a virtual row costs an
+// atomic fold and a row lookup, a window a 192 KiB copy and two barriers.
+// Swept on R-MAT scale 22 (0 - 5 per virtual row, 0 - 65536 per window; equal
+// entry shares ran 1.55x slower than these); Erdos-Renyi, whose cost is
+// uniform, is indifferent.  GBK_SEG_VROW_COST / GBK_SEG_WINDOW_COST override.
+constexpr double kVrowCost = 2.0;
+constexpr double kWindowCost = 16384.0;
+
+double env_weight(const char* name, double dflt) {
+    const char* e = std::getenv(name);
+    return e ? std::atof(e) : dflt;
+}
+
+// Cut the chunks into nsh shares of equal cost: share b is entries
+// [share[b], share[b + 1]), chunk aligned except the end (nnz).
+void split_shares(const std::vector<int32_t>& cvr, const std::vector<int32_t>& seg_start, int64_t nnz, int nsh,
+                  std::vector<int32_t>& share) {
+    const double wv = env_weight("GBK_SEG_VROW_COST", kVrowCost), ww = env_weight("GBK_SEG_WINDOW_COST", kWindowCost);
+    const int64_t nch = (int64_t)cvr.size() - 1;
+    // cost of the entries before chunk q: entries + virtual rows + windows begun
+    std::vector<double> cost(nch + 1);
+    size_t sg = 0;
+    int64_t begun = 0;  // non-empty segments starting at or before entry e
+    for (int64_t q = 0; q <= nch; ++q) {
+        const int64_t e = std::min<int64_t>(q * kChunk, nnz);
+        for (; sg + 1 < seg_start.size() && seg_start[sg] <= e; ++sg)
+            if (seg_start[sg] < seg_start[sg + 1]) ++begun;
+        cost[q] = (double)e + wv * (double)(cvr[q] + 1) + ww * (double)begun;
+    }
+    share.assign(nsh + 1, 0);
+    int64_t q = 0;
+    for (int b = 1; b < nsh; ++b) {
+        const double target = cost[nch] * b / nsh;
+        while (q < nch && cost[q] < target) ++q;
+        share[b] = (int32_t)std::min<int64_t>(q * kChunk, nnz);
+    }
+    share[nsh] = (int32_t)nnz;
+}
+
 template <typename T>
 int build_impl(const CsrView& a, SegSmem** out, cudaStream_t s) {
     SegSmem* f = new SegSmem();
@@ -293,17 +413,20 @@ int build_impl(const CsrView& a, SegSmem** out, cudaStream_t s) {
     f->ncols = a.ncols;
     f->nnz = a.nnz;
     f->nseg = (int32_t)std::max<int64_t>(1, (a.ncols + kSegCols - 1) / kSegCols);
-    const int64_t nnz = a.nnz, padded = ((nnz + 31) / 32) * 32 + 32;
+    const int64_t nnz = a.nnz;
+    f->nchunks = std::max<int64_t>(1, (nnz + kChunk - 1) / kChunk);
+    const int64_t padded = f->nchunks * kChunk, ngroups = f->nchunks * kGroups;
     auto fail = [&](int rc) {
         free_segsmem(f);
         return rc;
     };
-    if (cudaMalloc(&f->col, 2 * std::max<int64_t>(nnz, 1)) || cudaMalloc(&f->val, sizeof(T) * std::max<int64_t>(nnz, 1)) ||
-        cudaMalloc(&f->head, 4 * (padded / 32)) || cudaMalloc(&f->chunk_vr, 4 * (padded / 32)) ||
+    if (cudaMalloc(&f->col, 2 * padded) || cudaMalloc(&f->val, sizeof(T) * padded) ||
+        cudaMalloc(&f->grp, 2 * ngroups) || cudaMalloc(&f->cvr, 4 * (f->nchunks + 1)) ||
         cudaMalloc(&f->seg_start, 4 * (f->nseg + 1)) ||
         cudaMalloc(&f->tmp, sizeof(T) * std::max<int64_t>(a.nrows, 1)) || cudaMalloc(&f->err, 4))
         return fail(cuda_fail(cudaGetLastError(), "segmented format allocation", __FILE__, __LINE__));
-    if (cudaMemsetAsync(f->head, 0, 4 * (padded / 32), s) || cudaMemsetAsync(f->chunk_vr, 0, 4 * (padded / 32), s) ||
+    if (cudaMemsetAsync(f->col, 0, 2 * padded, s) || cudaMemsetAsync(f->val, 0, sizeof(T) * padded, s) ||
+        cudaMemsetAsync(f->grp, 0, 2 * ngroups, s) || cudaMemsetAsync(f->cvr, 0xff, 4 * (f->nchunks + 1), s) ||
         cudaMemsetAsync(f->err, 0, 4, s))
         return fail(cuda_fail(cudaGetLastError(), "cudaMemsetAsync", __FILE__, __LINE__));
     std::vector<int32_t> ss(f->nseg + 1, -1);
@@ -328,8 +451,8 @@ int build_impl(const CsrView& a, SegSmem** out, cudaStream_t s) {
         count_launch(1);
         GBK_CUDA(cudaMemsetAsync(f->seg_start, 0xff, 4 * (f->nseg + 1), s));
         GBK_CUDA(cudaMemsetAsync(flag + nnz, 0, 4, s));
-        k_ss_fill<T><<<blocks(padded), 256, 0, s>>>(keys2, pos2, a.idx, (const T*)a.val, nnz, padded, f->col,
-                                                    (T*)f->val, flag, f->head, f->seg_start);
+        k_ss_fill<T><<<blocks(nnz), 256, 0, s>>>(keys2, pos2, a.idx, (const T*)a.val, nnz, f->col, (T*)f->val, flag,
+                                                 f->seg_start);
         GBK_LAUNCHED();
         size_t sb = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, sb, flag, vid, (int)(nnz + 1), s);
@@ -343,7 +466,11 @@ int build_impl(const CsrView& a, SegSmem** out, cudaStream_t s) {
         GBK_CUDA(cudaStreamSynchronize(s));
         f->nvrows = nv;
         GBK_CUDA(cudaMalloc(&f->vrow, 4 * std::max<int64_t>(nv, 1)));
-        k_ss_vrows<<<blocks(nnz), 256, 0, s>>>(keys2, flag, vid, nnz, f->vrow, f->chunk_vr);
+        k_ss_vrows<<<blocks(nnz), 256, 0, s>>>(keys2, flag, vid, nnz, f->vrow);
+        GBK_LAUNCHED();
+        k_ss_groups<<<blocks(ngroups), 256, 0, s>>>(flag, vid, nnz, ngroups, f->grp);
+        GBK_LAUNCHED();
+        k_ss_cvr<<<blocks(f->nchunks + 1), 256, 0, s>>>(vid, nnz, f->nchunks, f->cvr);
         GBK_LAUNCHED();
         GBK_CUDA(cudaStreamSynchronize(s));
         cudaFree(stmp);
@@ -362,6 +489,14 @@ int build_impl(const CsrView& a, SegSmem** out, cudaStream_t s) {
     for (int32_t g = f->nseg - 1; g >= 0; --g)
         if (ss[g] < 0) ss[g] = ss[g + 1];
     GBK_CUDA(cudaMemcpyAsync(f->seg_start, ss.data(), 4 * (f->nseg + 1), cudaMemcpyHostToDevice, s));
+    // the CTAs' shares
+    std::vector<int32_t> cvr(f->nchunks + 1), share;
+    GBK_CUDA(cudaMemcpyAsync(cvr.data(), f->cvr, 4 * (f->nchunks + 1), cudaMemcpyDeviceToHost, s));
+    GBK_CUDA(cudaStreamSynchronize(s));
+    split_shares(cvr, ss, nnz, num_sms(), share);
+    f->nshares = (int32_t)share.size() - 1;
+    GBK_CUDA(cudaMalloc(&f->share, 4 * share.size()));
+    GBK_CUDA(cudaMemcpyAsync(f->share, share.data(), 4 * share.size(), cudaMemcpyHostToDevice, s));
     GBK_CUDA(cudaStreamSynchronize(s));
     *out = f;
     return GBK_SUCCESS;
@@ -382,9 +517,9 @@ int run_impl(const SegSmem* f, int accum, const T* x, T* y, cudaStream_t s) {
                                           (int)(kSegCols * sizeof(T))));
             attr = true;
         }
-        k_segsmem<SR, T><<<(unsigned)num_sms(), kSegThreads, kSegCols * sizeof(T), s>>>(
-            f->col, (const T*)f->val, f->head, f->chunk_vr, f->vrow, f->seg_start, f->nseg, f->nnz, f->ncols,
-            f->nvrows, f->nrows, x, out, f->err);
+        k_segsmem<SR, T><<<(unsigned)f->nshares, kSegThreads, kSegCols * sizeof(T), s>>>(
+            f->col, (const T*)f->val, f->grp, f->cvr, f->vrow, f->seg_start, f->share, f->nseg, f->ncols, f->nvrows,
+            f->nrows, x, out, f->err);
         GBK_LAUNCHED();
         if (f->check) {  // first call on this structure: confirm no index check fired
             int32_t e = 0;
@@ -437,10 +572,11 @@ void free_segsmem(SegSmem* f) {
     if (!f) return;
     cudaFree(f->col);
     cudaFree(f->val);
-    cudaFree(f->head);
-    cudaFree(f->chunk_vr);
+    cudaFree(f->grp);
+    cudaFree(f->cvr);
     cudaFree(f->vrow);
     cudaFree(f->seg_start);
+    cudaFree(f->share);
     cudaFree(f->tmp);
     cudaFree(f->err);
     delete f;
@@ -448,8 +584,8 @@ void free_segsmem(SegSmem* f) {
 
 size_t segsmem_bytes(const SegSmem* f) {
     if (!f) return 0;
-    return (size_t)f->nnz * 6 + (size_t)(f->nnz / 32 + 2) * 8 + (size_t)f->nvrows * 4 + (size_t)(f->nseg + 1) * 4 +
-           (size_t)f->nrows * 4;
+    return (size_t)f->nchunks * kChunk * 6 + (size_t)f->nchunks * kGroups * 2 + (size_t)(f->nchunks + 1) * 4 +
+           (size_t)f->nvrows * 4 + (size_t)(f->nseg + 1) * 4 + (size_t)(f->nshares + 1) * 4 + (size_t)f->nrows * 4;
 }
 
 }  // namespace gbk
