@@ -12,17 +12,20 @@
 //     8 l .. 8 l + 7 of a chunk, and a 16-bit group record per 8 entries holds
 //     their virtual-row start bits and the number of starts earlier in the
 //     chunk, so a lane knows its virtual rows without a scan;
-//   * 148 persistent CTAs (one per SM, 768 threads) take shares of whole
-//     chunks of equal estimated cost (entries, virtual rows and windows, each
-//     weighted by its measured cost); for each segment it touches a CTA copies
-//     that window of x into shared memory once (16-byte asynchronous copies),
-//     and its warps walk whole chunks: 16-byte column / value loads one chunk
-//     ahead, eight gathers from shared memory per lane, a sequential
-//     segmented sum per lane and ONE segmented warp scan per 256 entries for
-//     the virtual row that crosses lanes;
-//   * each virtual row's sum goes straight into y with one atomic of the
-//     semiring's add (float / int add, int / float minimum, or a store of 1
-//     for the logical-or semirings), so there is no merge pass.
+//   * 148 persistent CTAs (one per SM, 1024 threads) take shares of whole
+//     chunks of equal cost: first a model (entries, virtual rows and windows
+//     weighted by measured costs), then calibrated at build time from each
+//     CTA's timed share; for each segment it touches a CTA copies that window
+//     of x into shared memory once (asynchronous copies into bank-swizzled
+//     positions; the stored columns are already the swizzled positions);
+//   * its warps walk whole chunks: 16-byte column / value loads one chunk
+//     ahead, eight gathers from shared memory per lane, each lane's tail sum,
+//     ONE segmented warp scan per 256 entries for the runs that cross lanes,
+//     then a forward pass that writes every closed run's sum to a per-warp
+//     buffer in run order;
+//   * the warp folds those sums into y, 32 runs at a time, with one atomic of
+//     the semiring's add each (float / int add, int / float minimum, or a
+//     store of 1 for the logical-or semirings), so there is no merge pass.
 // Float sums therefore add in an order that varies between runs (within the
 // FP32 tolerance); integer and min / or results are exact.  Semirings whose
 // add is not associative fall back to the CSR kernels.
@@ -38,16 +41,27 @@
 namespace gbk {
 
 constexpr int kSegCols = 49152;  // x values per staged window (192 KiB of 4-byte values)
-constexpr int kSegThreads = 768;
+constexpr int kSegThreads = 1024;
 constexpr int kLaneEntries = 8;                  // entries per lane of a chunk
 constexpr int kChunk = 32 * kLaneEntries;        // entries per warp chunk
 constexpr int kGroups = kChunk / kLaneEntries;   // group records per chunk (one per lane)
+// dynamic shared memory of the SpMV kernel: the x window and one run-sum
+// buffer of a chunk per warp (4-byte values)
+constexpr size_t kSegSmemBytes = 4 * ((size_t)kSegCols + (size_t)(kSegThreads / 32) * kChunk);
+
+// Window position of column c (c < 65536) in shared memory: the column's
+// bank bits XOR the three higher 5-bit groups, a permutation inside each
+// 32-column block.  Power-law graphs put most entries on columns whose low
+// bits are zero; without the swizzle those all fall in bank 0.
+__host__ __device__ __forceinline__ uint32_t window_pos(uint32_t c) {
+    return c ^ (((c >> 5) ^ (c >> 10) ^ (c >> 15)) & 31u);
+}
 
 struct SegSmem {
     int64_t nrows = 0, ncols = 0, nnz = 0, nvrows = 0;
     int64_t nchunks = 0;
     int32_t nseg = 0;
-    uint16_t* col = nullptr;       // column inside the window, nchunks * kChunk (zero padded)
+    uint16_t* col = nullptr;       // window position of the column (window_pos), nchunks * kChunk (zero padded)
     void* val = nullptr;           // nchunks * kChunk (zero padded)
     uint16_t* grp = nullptr;       // per 8 entries: (virtual-row starts earlier in the chunk) << 8 | start bits
     int32_t* cvr = nullptr;        // nchunks + 1: virtual row open just before entry kChunk * q (-1 at 0)
@@ -82,7 +96,7 @@ __global__ void k_ss_fill(const unsigned long long* __restrict__ keys, const int
     const unsigned long long k = keys[i];
     const int32_t seg = (int32_t)(k >> 32);
     const int32_t e = pos[i];
-    col[i] = (uint16_t)(idx[e] - seg * kSegCols);
+    col[i] = (uint16_t)window_pos((uint32_t)(idx[e] - seg * kSegCols));
     val[i] = v[e];
     flag[i] = (i == 0) || (keys[i - 1] != k);
     if (i == 0 || (int32_t)(keys[i - 1] >> 32) != seg) seg_start[seg] = (int32_t)i;
@@ -191,50 +205,62 @@ template <> __device__ __forceinline__ int32_t from_bits<int32_t>(uint32_t u) { 
 // entries [a, b) (the first and last chunk may hold entries of a neighbouring
 // segment or of another CTA's share: those add the identity, but their
 // virtual-row starts still count, so the row numbering stays global).
+//
+// Per chunk: the lanes' products; each lane's tail (the sum after its last
+// start); a segmented warp scan of the tails gives the run coming into every
+// lane; a forward pass from that value gives the sum of every run a start
+// closes, which the lane writes to the warp's buffer at the run's index in the
+// chunk (run k of the chunk is virtual row cvr + k).  The warp then folds runs
+// lane, lane + 32, ... into y, their rows loaded at the start of the chunk.
+// Failed index checks are collected per lane and reported once at the end.
 template <int SR, typename T>
 __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, const uint4* __restrict__ val4,
                                                const uint16_t* __restrict__ grp, const int32_t* __restrict__ cvr,
-                                               const int32_t* __restrict__ vrow, const T* xs, int w, int64_t q0,
-                                               int64_t q1, int64_t a, int64_t b, T* out, int64_t nvrows,
-                                               int64_t nrows, int32_t* err) {
+                                               const int32_t* __restrict__ vrow, const T* xs, T* buf, int w,
+                                               int64_t q0, int64_t q1, int64_t a, int64_t b, T* out,
+                                               int64_t nvrows, int64_t nrows, int32_t* err) {
     using S = Semiring<SR, T>;
+    constexpr int kRowsAhead = 3;  // runs per lane whose rows are loaded at the start of a chunk
     const unsigned kAll = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned le = (lane == 31) ? kAll : ((2u << lane) - 1u);
-    const unsigned wl = (unsigned)(w - 1);  // last column of the window
+    const unsigned wl = (unsigned)(((w + 31) & ~31) - 1);  // last staged position of the window
     const unsigned wl2 = wl | (wl << 16);
+    const uint32_t nvr = (uint32_t)nvrows, nr = (uint32_t)nrows;  // both < 2^31
+    bool bad_col = false, bad_row = false;
     T carry = S::identity();  // the virtual row open at the end of the previous chunk
-    uint4 cn = __ldcs(col8 + q0 * kGroups + lane);
-    uint4 an = __ldcs(val4 + q0 * 2 * kGroups + 2 * lane);
-    uint4 bn = __ldcs(val4 + q0 * 2 * kGroups + 2 * lane + 1);
-    uint32_t gn = __ldcs(grp + q0 * kGroups + lane);
+    const uint4* pc = col8 + q0 * kGroups + lane;
+    const uint4* pv = val4 + q0 * 2 * kGroups + 2 * lane;
+    const uint16_t* pg = grp + q0 * kGroups + lane;
+    uint4 cn = __ldcs(pc), an = __ldcs(pv), bn = __ldcs(pv + 1);
+    uint32_t gn = __ldcs(pg);
     int32_t vn = __ldg(cvr + q0);
     for (int64_t q = q0; q < q1; ++q) {
         const uint4 c = cn, va = an, vb = bn;
         const uint32_t g = gn;
         const int32_t cv = vn;
         if (q + 1 < q1) {  // the next chunk's loads go out before this chunk's work
-            cn = __ldcs(col8 + (q + 1) * kGroups + lane);
-            an = __ldcs(val4 + (q + 1) * 2 * kGroups + 2 * lane);
-            bn = __ldcs(val4 + (q + 1) * 2 * kGroups + 2 * lane + 1);
-            gn = __ldcs(grp + (q + 1) * kGroups + lane);
+            pc += kGroups;
+            pv += 2 * kGroups;
+            pg += kGroups;
+            cn = __ldcs(pc);
+            an = __ldcs(pv);
+            bn = __ldcs(pv + 1);
+            gn = __ldcs(pg);
             vn = __ldg(cvr + q + 1);
         }
-        const uint32_t hb = g & 0xffu;                    // entries of this lane that start a virtual row
-        const int32_t vr_lane = cv + (int32_t)(g >> 8);   // virtual row open before this lane's entries
-        // rows of the virtual rows that end at this lane's starts (the i-th
-        // start closes virtual row vr_lane + number of starts before it)
-        int32_t r[kLaneEntries];
+        const uint32_t hb = g & 0xffu;      // entries of this lane that start a virtual row
+        const uint32_t before = g >> 8;     // starts in the chunk before this lane's entries
+        const int nrun = (int)__shfl_sync(kAll, before + __popc(hb), 31);  // runs the chunk closes
+        // rows of the first runs this lane folds
+        int32_t rr[kRowsAhead];
 #pragma unroll
-        for (int i = 0; i < kLaneEntries; ++i) {
-            r[i] = -1;
-            if ((hb >> i) & 1u) {
-                const int64_t vr = (int64_t)vr_lane + __popc(hb & ((1u << i) - 1u));
-                if (vr >= 0 && vr < nvrows) r[i] = __ldg(vrow + vr);
-            }
+        for (int k = 0; k < kRowsAhead; ++k) {
+            const uint32_t vr = (uint32_t)(cv + lane + 32 * k);
+            rr[k] = (lane + 32 * k < nrun && vr < nvr) ? __ldg(vrow + vr) : -1;
         }
         // a ragged chunk: entries outside [a, b) (another window's columns, or
-        // another share) read column 0 and add the identity
+        // another share) read position 0 and add the identity
         const int64_t cb = q * kChunk, e0 = cb + lane * kLaneEntries;
         const bool ragged = cb < a || cb + kChunk > b;
         uint32_t cr[4] = {c.x, c.y, c.z, c.w};
@@ -243,10 +269,10 @@ __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, c
             for (int i = 0; i < kLaneEntries; ++i)
                 if (e0 + i < a || e0 + i >= b) cr[i >> 1] &= (i & 1) ? 0x0000ffffu : 0xffff0000u;
         }
-        // products; columns are clamped into the window and a column outside
-        // it is reported
+        // products; positions are clamped into the window and one outside it
+        // is reported
         const uint32_t cmax = __vmaxu2(__vmaxu2(cr[0], cr[1]), __vmaxu2(cr[2], cr[3]));
-        if ((cmax & 0xffffu) > wl || (cmax >> 16) > wl) ss_flag(err, 1);
+        bad_col |= (cmax & 0xffffu) > wl || (cmax >> 16) > wl;
         const uint32_t vw[kLaneEntries] = {va.x, va.y, va.z, va.w, vb.x, vb.y, vb.z, vb.w};
         T p[kLaneEntries];
 #pragma unroll
@@ -260,59 +286,93 @@ __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, c
             for (int i = 0; i < kLaneEntries; ++i)
                 if (e0 + i < a || e0 + i >= b) p[i] = S::identity();
         }
-        // sequential segmented sum: em[i] is the run closed by a start at i
-        T em[kLaneEntries];
-        T acc = S::identity();
+        // this lane's tail: the entries from its last start on (all of them
+        // when it has none)
+        const int last = hb ? 31 - __clz(hb) : 0;
+        T tail = S::identity();
 #pragma unroll
-        for (int i = 0; i < kLaneEntries; ++i) {
-            em[i] = acc;
-            acc = ((hb >> i) & 1u) ? p[i] : S::add(acc, p[i]);
-        }
-        // segmented warp scan of the lane tails: s = the run open after this
-        // lane, including earlier lanes (and the previous chunk's carry) when
-        // no start lies between
+        for (int i = 0; i < kLaneEntries; ++i)
+            if (i >= last) tail = S::add(tail, p[i]);
+        // segmented warp scan of the tails: s = the run open after this lane,
+        // including earlier lanes (and the previous chunk's carry) when no
+        // start lies between
         const unsigned hle = __ballot_sync(kAll, hb != 0) & le;
         const int first = hle ? 31 - __clz(hle) : 0;  // last lane at or before this one with a start
-        T s = acc;
+        T s = tail;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
             const T o = __shfl_up_sync(kAll, s, d);
             if (lane - d >= first) s = S::add(s, o);
         }
         if (!hle) s = S::add(carry, s);
-        T xin = __shfl_up_sync(kAll, s, 1);  // the run open before this lane
-        if (lane == 0) xin = carry;
+        T acc = __shfl_up_sync(kAll, s, 1);  // the run open before this lane
+        if (lane == 0) acc = carry;
         carry = __shfl_sync(kAll, s, 31);
-        // fold the closed runs; the first start closes the run that came in
-        const int f = __ffs(hb) - 1;
+        // forward pass: a start at i closes the run summed so far; its sum
+        // goes to the buffer at the run's index in the chunk
+        T* slot = buf + before;
 #pragma unroll
-        for (int i = 0; i < kLaneEntries; ++i)
-            if ((hb >> i) & 1u) ss_emit<SR, T>(out, r[i], i == f ? S::add(xin, em[i]) : em[i], nrows, err);
+        for (int i = 0; i < kLaneEntries; ++i) {
+            if ((hb >> i) & 1u) {
+                *slot++ = acc;
+                acc = p[i];
+            } else {
+                acc = S::add(acc, p[i]);
+            }
+        }
+        __syncwarp();
+        // fold the runs the chunk closes
+#pragma unroll
+        for (int k = 0; k < kRowsAhead; ++k) {
+            const int j = lane + 32 * k;
+            if (j < nrun) {
+                const T v = buf[j];
+                if (changes<SR, T>(v)) {
+                    if ((uint32_t)rr[k] < nr)
+                        fold_into<SR, T>(out, rr[k], v);
+                    else
+                        bad_row = true;
+                }
+            }
+        }
+        for (int j = lane + 32 * kRowsAhead; j < nrun; j += 32) {  // chunks with more than 96 runs
+            const T v = buf[j];
+            if (changes<SR, T>(v)) {
+                const uint32_t vr = (uint32_t)(cv + j);
+                const int32_t r = vr < nvr ? __ldg(vrow + vr) : -1;
+                if ((uint32_t)r < nr)
+                    fold_into<SR, T>(out, r, v);
+                else
+                    bad_row = true;
+            }
+        }
+        __syncwarp();  // the buffer is read before the next chunk writes it
     }
     // the run still open after the last chunk
     if (lane == 0 && changes<SR, T>(carry)) {
-        const int32_t vr = __ldg(cvr + q1);
-        ss_emit<SR, T>(out, (vr >= 0 && vr < nvrows) ? __ldg(vrow + vr) : -1, carry, nrows, err);
+        const uint32_t vr = (uint32_t)__ldg(cvr + q1);
+        const int32_t r = vr < nvr ? __ldg(vrow + vr) : -1;
+        if ((uint32_t)r < nr)
+            fold_into<SR, T>(out, r, carry);
+        else
+            bad_row = true;
     }
+    if (bad_col) ss_flag(err, 1);
+    if (bad_row) ss_flag(err, 2);
 }
 
-// Copy w values of x into the shared window with 16-byte asynchronous copies
-// (all of a thread's copies in flight at once, no registers held), scalar
-// loads for a misaligned source and the last w % 4 values.  Returns once this
-// thread's copies have landed; the caller's barrier publishes them.
+// Copy w values of x into their swizzled shared-memory positions with 4-byte
+// asynchronous copies (all of a thread's copies in flight, no registers
+// held).  Returns once this thread's copies have landed; the caller's
+// barrier publishes them.
 template <typename T>
 __device__ __forceinline__ void stage_window(T* xs, const T* src, int w) {
-    int done = 0;
-    if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
-        const int n16 = w >> 2;
-        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(xs);
-        for (int i = threadIdx.x; i < n16; i += blockDim.x)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 16u * (uint32_t)i), "l"(src + 4 * i)
-                         : "memory");
-        asm volatile("cp.async.commit_group;" ::: "memory");
-        done = n16 * 4;
-    }
-    for (int i = done + threadIdx.x; i < w; i += blockDim.x) xs[i] = __ldg(src + i);
+    static_assert(sizeof(T) == 4, "4-byte values");
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(xs);
+    for (int i = threadIdx.x; i < w; i += blockDim.x)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst + 4u * window_pos((uint32_t)i)),
+                     "l"(src + i)
+                     : "memory");
     asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
@@ -321,12 +381,18 @@ __global__ void __launch_bounds__(kSegThreads, 1)
     k_segsmem(const uint16_t* __restrict__ col, const T* __restrict__ val, const uint16_t* __restrict__ grp,
               const int32_t* __restrict__ cvr, const int32_t* __restrict__ vrow,
               const int32_t* __restrict__ seg_start, const int32_t* __restrict__ share, int32_t nseg,
-              int64_t ncols, int64_t nvrows, int64_t nrows, const T* __restrict__ x, T* out, int32_t* err) {
+              int64_t ncols, int64_t nvrows, int64_t nrows, const T* __restrict__ x, T* out, int32_t* err,
+              long long* clk) {
     extern __shared__ __align__(16) unsigned char ss_smem[];
     T* xs = reinterpret_cast<T*>(ss_smem);
     const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    T* buf = xs + kSegCols + warp * kChunk;  // this warp's run sums
+    const long long t0 = clock64();
     const int64_t c0 = share[blockIdx.x], c1 = share[blockIdx.x + 1];
-    if (c0 >= c1) return;  // the whole block leaves together
+    if (c0 >= c1) {  // the whole block leaves together
+        if (clk && threadIdx.x == 0) clk[blockIdx.x] = 0;
+        return;
+    }
     int lo = 0, hi = nseg;  // last segment starting at or before c0
     while (hi - lo > 1) {
         const int mid = (lo + hi) >> 1;
@@ -349,8 +415,27 @@ __global__ void __launch_bounds__(kSegThreads, 1)
         const int64_t per = (qb - qa + nwarps - 1) / nwarps;
         const int64_t q0 = qa + (int64_t)warp * per, q1 = min(qb, q0 + per);
         if (q0 < q1)
-            ss_warp_chunks<SR, T>(col8, val4, grp, cvr, vrow, xs, w, q0, q1, a, b, out, nvrows, nrows, err);
+            ss_warp_chunks<SR, T>(col8, val4, grp, cvr, vrow, xs, buf, w, q0, q1, a, b, out, nvrows, nrows, err);
     }
+    if (clk) {  // calibration launches: the block's time in SM cycles
+        __syncthreads();
+        if (threadIdx.x == 0) clk[blockIdx.x] = clock64() - t0;
+    }
+}
+
+template <int SR, typename T>
+int launch_segsmem(const SegSmem* f, const T* x, T* out, long long* clk, cudaStream_t s) {
+    static bool attr = false;  // one per instantiation
+    if (!attr) {
+        GBK_CUDA(cudaFuncSetAttribute(k_segsmem<SR, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kSegSmemBytes));
+        attr = true;
+    }
+    k_segsmem<SR, T><<<(unsigned)f->nshares, kSegThreads, kSegSmemBytes, s>>>(
+        f->col, (const T*)f->val, f->grp, f->cvr, f->vrow, f->seg_start, f->share, f->nseg, f->ncols, f->nvrows,
+        f->nrows, x, out, f->err, clk);
+    GBK_LAUNCHED();
+    return GBK_SUCCESS;
 }
 
 template <typename T>
@@ -380,13 +465,11 @@ double env_weight(const char* name, double dflt) {
     return e ? std::atof(e) : dflt;
 }
 
-// Cut the chunks into nsh shares of equal cost: share b is entries
-// [share[b], share[b + 1]), chunk aligned except the end (nnz).
-void split_shares(const std::vector<int32_t>& cvr, const std::vector<int32_t>& seg_start, int64_t nnz, int nsh,
-                  std::vector<int32_t>& share) {
+// Modelled cost of the entries before chunk q (q = 0 .. nchunks): entries +
+// virtual rows + windows begun, in entries.
+std::vector<double> model_cost(const std::vector<int32_t>& cvr, const std::vector<int32_t>& seg_start, int64_t nnz) {
     const double wv = env_weight("GBK_SEG_VROW_COST", kVrowCost), ww = env_weight("GBK_SEG_WINDOW_COST", kWindowCost);
     const int64_t nch = (int64_t)cvr.size() - 1;
-    // cost of the entries before chunk q: entries + virtual rows + windows begun
     std::vector<double> cost(nch + 1);
     size_t sg = 0;
     int64_t begun = 0;  // non-empty segments starting at or before entry e
@@ -396,14 +479,74 @@ void split_shares(const std::vector<int32_t>& cvr, const std::vector<int32_t>& s
             if (seg_start[sg] < seg_start[sg + 1]) ++begun;
         cost[q] = (double)e + wv * (double)(cvr[q] + 1) + ww * (double)begun;
     }
+    return cost;
+}
+
+// Cut the chunks into nsh shares of equal weight (w: non-decreasing weight of
+// the chunks before q): share b is entries [share[b], share[b + 1]), chunk
+// aligned except the end (nnz).
+void cut_shares(const std::vector<double>& w, int64_t nnz, int nsh, std::vector<int32_t>& share) {
+    const int64_t nch = (int64_t)w.size() - 1;
     share.assign(nsh + 1, 0);
     int64_t q = 0;
     for (int b = 1; b < nsh; ++b) {
-        const double target = cost[nch] * b / nsh;
-        while (q < nch && cost[q] < target) ++q;
+        const double target = w[nch] * b / nsh;
+        while (q < nch && w[q] < target) ++q;
         share[b] = (int32_t)std::min<int64_t>(q * kChunk, nnz);
     }
     share[nsh] = (int32_t)nnz;
+}
+
+// Calibrated shares: time every CTA's share (plus-times over x = 1, SM
+// cycles), spread each share's time over its chunks by the modelled cost and
+// cut again at equal time; a few rounds settle it.  The model alone leaves
+// the slowest CTA 1.2 - 1.5x above the mean on power-law graphs.
+constexpr int kCalibrationRounds = 3;
+
+int calibrate_shares(SegSmem* f, const std::vector<double>& cost, std::vector<int32_t>& share, cudaStream_t s) {
+    const int nsh = f->nshares;
+    const int64_t nch = (int64_t)cost.size() - 1;
+    float* x1 = nullptr;
+    long long* clk = nullptr;
+    GBK_CUDA(cudaMalloc(&x1, sizeof(float) * std::max<int64_t>(f->ncols, 1)));
+    GBK_CUDA(cudaMalloc(&clk, sizeof(long long) * nsh));
+    k_ss_init<float><<<blocks(f->ncols), 256, 0, s>>>(x1, f->ncols, 1.0f);
+    GBK_LAUNCHED();
+    std::vector<long long> t(nsh);
+    std::vector<double> w(nch + 1);
+    int rc = GBK_SUCCESS;
+    for (int round = 0; round < kCalibrationRounds && rc == GBK_SUCCESS; ++round) {
+        for (int rep = 0; rep < 2 && rc == GBK_SUCCESS; ++rep)  // the second launch is timed warm
+            rc = launch_segsmem<GBK_PLUS_TIMES, float>(f, x1, (float*)f->tmp, clk, s);
+        if (rc != GBK_SUCCESS) break;
+        GBK_CUDA(cudaMemcpyAsync(t.data(), clk, sizeof(long long) * nsh, cudaMemcpyDeviceToHost, s));
+        GBK_CUDA(cudaStreamSynchronize(s));
+        double tsum = 0, csum = 0;
+        for (int b = 0; b < nsh; ++b) {
+            const int64_t q0 = (share[b] + kChunk - 1) / kChunk, q1 = (share[b + 1] + kChunk - 1) / kChunk;
+            if (q1 > q0 && t[b] > 0) {
+                tsum += (double)t[b];
+                csum += cost[q1] - cost[q0];
+            }
+        }
+        if (tsum <= 0 || csum <= 0) break;
+        double acc = 0;
+        w[0] = 0;
+        for (int b = 0; b < nsh; ++b) {
+            const int64_t q0 = (share[b] + kChunk - 1) / kChunk, q1 = (share[b + 1] + kChunk - 1) / kChunk;
+            if (q1 <= q0) continue;
+            const double cb = cost[q1] - cost[q0];
+            const double tb = t[b] > 0 ? (double)t[b] : cb * tsum / csum;
+            for (int64_t q = q0 + 1; q <= q1; ++q) w[q] = acc + tb * (cost[q] - cost[q0]) / cb;
+            acc += tb;
+        }
+        cut_shares(w, f->nnz, nsh, share);
+        GBK_CUDA(cudaMemcpyAsync(f->share, share.data(), 4 * share.size(), cudaMemcpyHostToDevice, s));
+    }
+    GBK_CUDA(cudaStreamSynchronize(s));
+    cudaFree(x1);
+    cudaFree(clk);
+    return rc;
 }
 
 template <typename T>
@@ -493,11 +636,17 @@ int build_impl(const CsrView& a, SegSmem** out, cudaStream_t s) {
     std::vector<int32_t> cvr(f->nchunks + 1), share;
     GBK_CUDA(cudaMemcpyAsync(cvr.data(), f->cvr, 4 * (f->nchunks + 1), cudaMemcpyDeviceToHost, s));
     GBK_CUDA(cudaStreamSynchronize(s));
-    split_shares(cvr, ss, nnz, num_sms(), share);
+    const std::vector<double> cost = model_cost(cvr, ss, nnz);
+    cut_shares(cost, nnz, num_sms(), share);
     f->nshares = (int32_t)share.size() - 1;
     GBK_CUDA(cudaMalloc(&f->share, 4 * share.size()));
     GBK_CUDA(cudaMemcpyAsync(f->share, share.data(), 4 * share.size(), cudaMemcpyHostToDevice, s));
     GBK_CUDA(cudaStreamSynchronize(s));
+    if (std::is_same<T, float>::value && nnz > 0) {
+        const int rc = calibrate_shares(f, cost, share, s);
+        if (rc != GBK_SUCCESS) return fail(rc);
+        GBK_CUDA(cudaMemsetAsync(f->err, 0, 4, s));
+    }
     *out = f;
     return GBK_SUCCESS;
 }
@@ -511,16 +660,8 @@ int run_impl(const SegSmem* f, int accum, const T* x, T* y, cudaStream_t s) {
         GBK_LAUNCHED();
     }
     if (f->nnz > 0) {
-        static bool attr = false;  // one per instantiation
-        if (!attr) {
-            GBK_CUDA(cudaFuncSetAttribute(k_segsmem<SR, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)(kSegCols * sizeof(T))));
-            attr = true;
-        }
-        k_segsmem<SR, T><<<(unsigned)f->nshares, kSegThreads, kSegCols * sizeof(T), s>>>(
-            f->col, (const T*)f->val, f->grp, f->cvr, f->vrow, f->seg_start, f->share, f->nseg, f->ncols, f->nvrows,
-            f->nrows, x, out, f->err);
-        GBK_LAUNCHED();
+        const int rc = launch_segsmem<SR, T>(f, x, out, nullptr, s);
+        if (rc != GBK_SUCCESS) return rc;
         if (f->check) {  // first call on this structure: confirm no index check fired
             int32_t e = 0;
             GBK_CUDA(cudaMemcpyAsync(&e, f->err, 4, cudaMemcpyDeviceToHost, s));
