@@ -45,9 +45,12 @@ constexpr int kSegThreads = 1024;
 constexpr int kLaneEntries = 8;                  // entries per lane of a chunk
 constexpr int kChunk = 32 * kLaneEntries;        // entries per warp chunk
 constexpr int kGroups = kChunk / kLaneEntries;   // group records per chunk (one per lane)
+// run sums of one chunk: up to kChunk closed runs and the one left open,
+// padded to 16 bytes
+constexpr int kRunSlots = kChunk + 8;
 // dynamic shared memory of the SpMV kernel: the x window and one run-sum
-// buffer of a chunk per warp (4-byte values)
-constexpr size_t kSegSmemBytes = 4 * ((size_t)kSegCols + (size_t)(kSegThreads / 32) * kChunk);
+// buffer per warp (4-byte values)
+constexpr size_t kSegSmemBytes = 4 * ((size_t)kSegCols + (size_t)(kSegThreads / 32) * kRunSlots);
 
 // Window position of column c (c < 65536) in shared memory: the column's
 // bank bits XOR the three higher 5-bit groups, a permutation inside each
@@ -201,23 +204,26 @@ template <typename T> __device__ __forceinline__ T from_bits(uint32_t u);
 template <> __device__ __forceinline__ float from_bits<float>(uint32_t u) { return __uint_as_float(u); }
 template <> __device__ __forceinline__ int32_t from_bits<int32_t>(uint32_t u) { return (int32_t)u; }
 
-// One warp over chunks [q0, q1) of the staged segment, restricted to the
-// entries [a, b) (the first and last chunk may hold entries of a neighbouring
-// segment or of another CTA's share: those add the identity, but their
-// virtual-row starts still count, so the row numbering stays global).
+// One warp's share of the chunks [qa, qb) of the staged segment, restricted
+// to the entries [a, b) (the first and last chunk may hold entries of a
+// neighbouring segment or of another CTA's share: those add the identity, but
+// their virtual-row starts still count, so the row numbering stays global).
+// The warps of the CTA take chunks one at a time from a shared counter, so a
+// warp with costly chunks does not hold the others at the next window.
 //
-// Per chunk: the lanes' products; each lane's tail (the sum after its last
-// start); a segmented warp scan of the tails gives the run coming into every
-// lane; a forward pass from that value gives the sum of every run a start
-// closes, which the lane writes to the warp's buffer at the run's index in the
-// chunk (run k of the chunk is virtual row cvr + k).  The warp then folds runs
+// Every chunk stands alone: the lanes' products; each lane's tail (the sum
+// after its last start); a segmented warp scan of the tails gives the run
+// coming into every lane; a forward pass from that value gives the sum of
+// every run a start closes, which the lane writes to the warp's buffer at the
+// run's index in the chunk (run k of the chunk is virtual row cvr + k; the
+// run still open at the chunk's end is run nrun).  The warp then folds runs
 // lane, lane + 32, ... into y, their rows loaded at the start of the chunk.
 // Failed index checks are collected per lane and reported once at the end.
 template <int SR, typename T>
 __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, const uint4* __restrict__ val4,
                                                const uint16_t* __restrict__ grp, const int32_t* __restrict__ cvr,
                                                const int32_t* __restrict__ vrow, const T* xs, T* buf, int w,
-                                               int64_t q0, int64_t q1, int64_t a, int64_t b, T* out,
+                                               int64_t qa, int64_t qb, int64_t a, int64_t b, int* next, T* out,
                                                int64_t nvrows, int64_t nrows, int32_t* err) {
     using S = Semiring<SR, T>;
     constexpr int kRowsAhead = 3;  // runs per lane whose rows are loaded at the start of a chunk
@@ -228,36 +234,38 @@ __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, c
     const unsigned wl2 = wl | (wl << 16);
     const uint32_t nvr = (uint32_t)nvrows, nr = (uint32_t)nrows;  // both < 2^31
     bool bad_col = false, bad_row = false;
-    T carry = S::identity();  // the virtual row open at the end of the previous chunk
-    const uint4* pc = col8 + q0 * kGroups + lane;
-    const uint4* pv = val4 + q0 * 2 * kGroups + 2 * lane;
-    const uint16_t* pg = grp + q0 * kGroups + lane;
-    uint4 cn = __ldcs(pc), an = __ldcs(pv), bn = __ldcs(pv + 1);
-    uint32_t gn = __ldcs(pg);
-    int32_t vn = __ldg(cvr + q0);
-    for (int64_t q = q0; q < q1; ++q) {
+    auto grab = [&]() -> int64_t {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(next, 1);
+        return qa + __shfl_sync(kAll, t, 0);
+    };
+    int64_t q = grab();
+    if (q >= qb) return;
+    uint4 cn = __ldcs(col8 + q * kGroups + lane);
+    uint4 an = __ldcs(val4 + q * 2 * kGroups + 2 * lane), bn = __ldcs(val4 + q * 2 * kGroups + 2 * lane + 1);
+    uint32_t gn = __ldcs(grp + q * kGroups + lane);
+    int32_t vn = __ldg(cvr + q);
+    for (;;) {
+        const int64_t qn = grab();
         const uint4 c = cn, va = an, vb = bn;
         const uint32_t g = gn;
         const int32_t cv = vn;
-        if (q + 1 < q1) {  // the next chunk's loads go out before this chunk's work
-            pc += kGroups;
-            pv += 2 * kGroups;
-            pg += kGroups;
-            cn = __ldcs(pc);
-            an = __ldcs(pv);
-            bn = __ldcs(pv + 1);
-            gn = __ldcs(pg);
-            vn = __ldg(cvr + q + 1);
+        if (qn < qb) {  // the next chunk's loads go out before this chunk's work
+            cn = __ldcs(col8 + qn * kGroups + lane);
+            an = __ldcs(val4 + qn * 2 * kGroups + 2 * lane);
+            bn = __ldcs(val4 + qn * 2 * kGroups + 2 * lane + 1);
+            gn = __ldcs(grp + qn * kGroups + lane);
+            vn = __ldg(cvr + qn);
         }
         const uint32_t hb = g & 0xffu;      // entries of this lane that start a virtual row
         const uint32_t before = g >> 8;     // starts in the chunk before this lane's entries
-        const int nrun = (int)__shfl_sync(kAll, before + __popc(hb), 31);  // runs the chunk closes
-        // rows of the first runs this lane folds
+        const int nrun = (int)__shfl_sync(kAll, before + __popc(hb), 31);  // runs the chunk's starts close
+        // rows of the first runs this lane folds (runs 0 .. nrun)
         int32_t rr[kRowsAhead];
 #pragma unroll
         for (int k = 0; k < kRowsAhead; ++k) {
             const uint32_t vr = (uint32_t)(cv + lane + 32 * k);
-            rr[k] = (lane + 32 * k < nrun && vr < nvr) ? __ldg(vrow + vr) : -1;
+            rr[k] = (lane + 32 * k <= nrun && vr < nvr) ? __ldg(vrow + vr) : -1;
         }
         // a ragged chunk: entries outside [a, b) (another window's columns, or
         // another share) read position 0 and add the identity
@@ -294,8 +302,7 @@ __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, c
         for (int i = 0; i < kLaneEntries; ++i)
             if (i >= last) tail = S::add(tail, p[i]);
         // segmented warp scan of the tails: s = the run open after this lane,
-        // including earlier lanes (and the previous chunk's carry) when no
-        // start lies between
+        // including earlier lanes when no start lies between
         const unsigned hle = __ballot_sync(kAll, hb != 0) & le;
         const int first = hle ? 31 - __clz(hle) : 0;  // last lane at or before this one with a start
         T s = tail;
@@ -304,10 +311,8 @@ __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, c
             const T o = __shfl_up_sync(kAll, s, d);
             if (lane - d >= first) s = S::add(s, o);
         }
-        if (!hle) s = S::add(carry, s);
         T acc = __shfl_up_sync(kAll, s, 1);  // the run open before this lane
-        if (lane == 0) acc = carry;
-        carry = __shfl_sync(kAll, s, 31);
+        if (lane == 0) acc = S::identity();
         // forward pass: a start at i closes the run summed so far; its sum
         // goes to the buffer at the run's index in the chunk
         T* slot = buf + before;
@@ -320,12 +325,13 @@ __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, c
                 acc = S::add(acc, p[i]);
             }
         }
+        if (lane == 31) *slot = acc;  // the run open at the chunk's end (slot = buf + nrun)
         __syncwarp();
-        // fold the runs the chunk closes
+        // fold the runs
 #pragma unroll
         for (int k = 0; k < kRowsAhead; ++k) {
             const int j = lane + 32 * k;
-            if (j < nrun) {
+            if (j <= nrun) {
                 const T v = buf[j];
                 if (changes<SR, T>(v)) {
                     if ((uint32_t)rr[k] < nr)
@@ -335,7 +341,7 @@ __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, c
                 }
             }
         }
-        for (int j = lane + 32 * kRowsAhead; j < nrun; j += 32) {  // chunks with more than 96 runs
+        for (int j = lane + 32 * kRowsAhead; j <= nrun; j += 32) {  // chunks with 96 runs or more
             const T v = buf[j];
             if (changes<SR, T>(v)) {
                 const uint32_t vr = (uint32_t)(cv + j);
@@ -347,15 +353,8 @@ __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, c
             }
         }
         __syncwarp();  // the buffer is read before the next chunk writes it
-    }
-    // the run still open after the last chunk
-    if (lane == 0 && changes<SR, T>(carry)) {
-        const uint32_t vr = (uint32_t)__ldg(cvr + q1);
-        const int32_t r = vr < nvr ? __ldg(vrow + vr) : -1;
-        if ((uint32_t)r < nr)
-            fold_into<SR, T>(out, r, carry);
-        else
-            bad_row = true;
+        if (qn >= qb) break;
+        q = qn;
     }
     if (bad_col) ss_flag(err, 1);
     if (bad_row) ss_flag(err, 2);
@@ -385,8 +384,9 @@ __global__ void __launch_bounds__(kSegThreads, 1)
               long long* clk) {
     extern __shared__ __align__(16) unsigned char ss_smem[];
     T* xs = reinterpret_cast<T*>(ss_smem);
-    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    T* buf = xs + kSegCols + warp * kChunk;  // this warp's run sums
+    const int warp = threadIdx.x >> 5;
+    T* buf = xs + kSegCols + warp * kRunSlots;  // this warp's run sums
+    __shared__ int next_chunk;                  // chunks of the segment part handed out so far
     const long long t0 = clock64();
     const int64_t c0 = share[blockIdx.x], c1 = share[blockIdx.x + 1];
     if (c0 >= c1) {  // the whole block leaves together
@@ -407,15 +407,14 @@ __global__ void __launch_bounds__(kSegThreads, 1)
         const int64_t a = max(c0, (int64_t)seg_start[s]), b = min(c1, (int64_t)seg_start[s + 1]);
         if (a >= b) continue;
         __syncthreads();  // the previous window's readers are done
+        if (threadIdx.x == 0) next_chunk = 0;
         const int64_t col0 = (int64_t)s * kSegCols;
         const int w = (int)min((int64_t)kSegCols, ncols - col0);
         stage_window(xs, x + col0, w);
         __syncthreads();
         const int64_t qa = a / kChunk, qb = (b + kChunk - 1) / kChunk;
-        const int64_t per = (qb - qa + nwarps - 1) / nwarps;
-        const int64_t q0 = qa + (int64_t)warp * per, q1 = min(qb, q0 + per);
-        if (q0 < q1)
-            ss_warp_chunks<SR, T>(col8, val4, grp, cvr, vrow, xs, buf, w, q0, q1, a, b, out, nvrows, nrows, err);
+        ss_warp_chunks<SR, T>(col8, val4, grp, cvr, vrow, xs, buf, w, qa, qb, a, b, &next_chunk, out, nvrows, nrows,
+                              err);
     }
     if (clk) {  // calibration launches: the block's time in SM cycles
         __syncthreads();
