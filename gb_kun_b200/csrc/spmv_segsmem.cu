@@ -234,23 +234,25 @@ __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, c
     const unsigned wl2 = wl | (wl << 16);
     const uint32_t nvr = (uint32_t)nvrows, nr = (uint32_t)nrows;  // both < 2^31
     bool bad_col = false, bad_row = false;
-    auto grab = [&]() -> int64_t {
+    // chunk and entry numbers fit 32 bits (nnz < 2^31)
+    const int32_t qa32 = (int32_t)qa, qb32 = (int32_t)qb, a32 = (int32_t)a, b32 = (int32_t)b;
+    auto grab = [&]() -> int32_t {
         int t = 0;
         if (lane == 0) t = atomicAdd(next, 1);
-        return qa + __shfl_sync(kAll, t, 0);
+        return qa32 + __shfl_sync(kAll, t, 0);
     };
-    int64_t q = grab();
-    if (q >= qb) return;
+    int32_t q = grab();
+    if (q >= qb32) return;
     uint4 cn = __ldcs(col8 + q * kGroups + lane);
     uint4 an = __ldcs(val4 + q * 2 * kGroups + 2 * lane), bn = __ldcs(val4 + q * 2 * kGroups + 2 * lane + 1);
     uint32_t gn = __ldcs(grp + q * kGroups + lane);
     int32_t vn = __ldg(cvr + q);
     for (;;) {
-        const int64_t qn = grab();
+        const int32_t qn = grab();
         const uint4 c = cn, va = an, vb = bn;
         const uint32_t g = gn;
         const int32_t cv = vn;
-        if (qn < qb) {  // the next chunk's loads go out before this chunk's work
+        if (qn < qb32) {  // the next chunk's loads go out before this chunk's work
             cn = __ldcs(col8 + qn * kGroups + lane);
             an = __ldcs(val4 + qn * 2 * kGroups + 2 * lane);
             bn = __ldcs(val4 + qn * 2 * kGroups + 2 * lane + 1);
@@ -269,13 +271,13 @@ __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, c
         }
         // a ragged chunk: entries outside [a, b) (another window's columns, or
         // another share) read position 0 and add the identity
-        const int64_t cb = q * kChunk, e0 = cb + lane * kLaneEntries;
-        const bool ragged = cb < a || cb + kChunk > b;
+        const int32_t cb = q * kChunk, e0 = cb + lane * kLaneEntries;
+        const bool ragged = cb < a32 || cb + kChunk > b32;
         uint32_t cr[4] = {c.x, c.y, c.z, c.w};
         if (ragged) {
 #pragma unroll
             for (int i = 0; i < kLaneEntries; ++i)
-                if (e0 + i < a || e0 + i >= b) cr[i >> 1] &= (i & 1) ? 0x0000ffffu : 0xffff0000u;
+                if (e0 + i < a32 || e0 + i >= b32) cr[i >> 1] &= (i & 1) ? 0x0000ffffu : 0xffff0000u;
         }
         // products; positions are clamped into the window and one outside it
         // is reported
@@ -292,7 +294,7 @@ __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, c
         if (ragged) {
 #pragma unroll
             for (int i = 0; i < kLaneEntries; ++i)
-                if (e0 + i < a || e0 + i >= b) p[i] = S::identity();
+                if (e0 + i < a32 || e0 + i >= b32) p[i] = S::identity();
         }
         // this lane's tail: the entries from its last start on (all of them
         // when it has none)
@@ -329,17 +331,13 @@ __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, c
         __syncwarp();
         // fold the runs
 #pragma unroll
-        for (int k = 0; k < kRowsAhead; ++k) {
+        for (int k = 0; k < kRowsAhead; ++k) {  // (slots past nrun hold stale sums and fold nothing)
             const int j = lane + 32 * k;
-            if (j <= nrun) {
-                const T v = buf[j];
-                if (changes<SR, T>(v)) {
-                    if ((uint32_t)rr[k] < nr)
-                        fold_into<SR, T>(out, rr[k], v);
-                    else
-                        bad_row = true;
-                }
-            }
+            const T v = buf[j];
+            const bool fold = j <= nrun && changes<SR, T>(v);
+            const bool ok = (uint32_t)rr[k] < nr;
+            if (fold && ok) fold_into<SR, T>(out, rr[k], v);
+            bad_row |= fold && !ok;
         }
         for (int j = lane + 32 * kRowsAhead; j <= nrun; j += 32) {  // chunks with 96 runs or more
             const T v = buf[j];
@@ -353,7 +351,7 @@ __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, c
             }
         }
         __syncwarp();  // the buffer is read before the next chunk writes it
-        if (qn >= qb) break;
+        if (qn >= qb32) break;
         q = qn;
     }
     if (bad_col) ss_flag(err, 1);
@@ -441,6 +439,24 @@ template <typename T>
 __global__ void k_ss_init(T* out, int64_t n, T v) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = v;
+}
+
+// y = the add's identity before the folds: grid-stride 16-byte stores (the
+// caller's y may be only 4-byte aligned: the head and tail go one by one)
+template <typename T>
+__global__ void k_ss_identity(T* __restrict__ out, int64_t n, T v) {
+    const int64_t lead = (int64_t)((16 - (reinterpret_cast<uintptr_t>(out) & 15)) & 15) / 4;
+    const int64_t head = lead < n ? lead : n;
+    const int64_t n4 = (n - head) / 4;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint4 w;
+    w.x = w.y = w.z = w.w = *reinterpret_cast<const uint32_t*>(&v);
+    uint4* o4 = reinterpret_cast<uint4*>(out + head);
+    for (int64_t i = t; i < n4; i += stride) o4[i] = w;
+    if (t < head) out[t] = v;
+    const int64_t tail = head + 4 * n4 + t;
+    if (tail < n) out[tail] = v;
 }
 
 template <typename T>
@@ -655,7 +671,8 @@ int run_impl(const SegSmem* f, int accum, const T* x, T* y, cudaStream_t s) {
     using S = Semiring<SR, T>;
     T* out = accum == GBK_OP_SECOND ? y : (T*)f->tmp;
     if (f->nrows > 0) {
-        k_ss_init<T><<<blocks(f->nrows), 256, 0, s>>>(out, f->nrows, S::identity());
+        const unsigned nb = (unsigned)std::min<int64_t>((f->nrows / 4 + 255) / 256 + 1, 8 * num_sms());
+        k_ss_identity<T><<<nb, 256, 0, s>>>(out, f->nrows, S::identity());
         GBK_LAUNCHED();
     }
     if (f->nnz > 0) {
