@@ -410,6 +410,10 @@ __global__ void __launch_bounds__(kSegThreads, 1)
         const int w = (int)min((int64_t)kSegCols, ncols - col0);
         stage_window(xs, x + col0, w);
         __syncthreads();
+        // y's initialisation (the kernel before this one on the stream) has
+        // finished before the first fold.  Launched with programmatic stream
+        // serialisation, everything above overlaps it; otherwise a no-op.
+        asm volatile("griddepcontrol.wait;" ::: "memory");
         const int64_t qa = a / kChunk, qb = (b + kChunk - 1) / kChunk;
         ss_warp_chunks<SR, T>(col8, val4, grp, cvr, vrow, xs, buf, w, qa, qb, a, b, &next_chunk, out, nvrows, nrows,
                               err);
@@ -421,16 +425,30 @@ __global__ void __launch_bounds__(kSegThreads, 1)
 }
 
 template <int SR, typename T>
-int launch_segsmem(const SegSmem* f, const T* x, T* out, long long* clk, cudaStream_t s) {
+// overlap_prev: the kernel before this launch on the stream is y's
+// initialisation, which calls griddepcontrol.launch_dependents; this launch
+// may then start (and stage its first window) while it runs.
+int launch_segsmem(const SegSmem* f, const T* x, T* out, long long* clk, bool overlap_prev, cudaStream_t s) {
     static bool attr = false;  // one per instantiation
     if (!attr) {
         GBK_CUDA(cudaFuncSetAttribute(k_segsmem<SR, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kSegSmemBytes));
         attr = true;
     }
-    k_segsmem<SR, T><<<(unsigned)f->nshares, kSegThreads, kSegSmemBytes, s>>>(
-        f->col, (const T*)f->val, f->grp, f->cvr, f->vrow, f->seg_start, f->share, f->nseg, f->ncols, f->nvrows,
-        f->nrows, x, out, f->err, clk);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)f->nshares);
+    cfg.blockDim = dim3(kSegThreads);
+    cfg.dynamicSmemBytes = kSegSmemBytes;
+    cfg.stream = s;
+    cudaLaunchAttribute la[1];
+    la[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    la[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = la;
+    cfg.numAttrs = overlap_prev ? 1 : 0;
+    GBK_CUDA(cudaLaunchKernelEx(&cfg, k_segsmem<SR, T>, (const uint16_t*)f->col, (const T*)f->val,
+                                (const uint16_t*)f->grp, (const int32_t*)f->cvr, (const int32_t*)f->vrow,
+                                (const int32_t*)f->seg_start, (const int32_t*)f->share, f->nseg, f->ncols, f->nvrows,
+                                f->nrows, x, out, f->err, clk));
     GBK_LAUNCHED();
     return GBK_SUCCESS;
 }
@@ -445,6 +463,7 @@ __global__ void k_ss_init(T* out, int64_t n, T v) {
 // caller's y may be only 4-byte aligned: the head and tail go one by one)
 template <typename T>
 __global__ void k_ss_identity(T* __restrict__ out, int64_t n, T v) {
+    asm volatile("griddepcontrol.launch_dependents;");  // the SpMV kernel may start its prologue
     const int64_t lead = (int64_t)((16 - (reinterpret_cast<uintptr_t>(out) & 15)) & 15) / 4;
     const int64_t head = lead < n ? lead : n;
     const int64_t n4 = (n - head) / 4;
@@ -532,7 +551,7 @@ int calibrate_shares(SegSmem* f, const std::vector<double>& cost, std::vector<in
     int rc = GBK_SUCCESS;
     for (int round = 0; round < kCalibrationRounds && rc == GBK_SUCCESS; ++round) {
         for (int rep = 0; rep < 2 && rc == GBK_SUCCESS; ++rep)  // the second launch is timed warm
-            rc = launch_segsmem<GBK_PLUS_TIMES, float>(f, x1, (float*)f->tmp, clk, s);
+            rc = launch_segsmem<GBK_PLUS_TIMES, float>(f, x1, (float*)f->tmp, clk, false, s);
         if (rc != GBK_SUCCESS) break;
         GBK_CUDA(cudaMemcpyAsync(t.data(), clk, sizeof(long long) * nsh, cudaMemcpyDeviceToHost, s));
         GBK_CUDA(cudaStreamSynchronize(s));
@@ -676,7 +695,7 @@ int run_impl(const SegSmem* f, int accum, const T* x, T* y, cudaStream_t s) {
         GBK_LAUNCHED();
     }
     if (f->nnz > 0) {
-        const int rc = launch_segsmem<SR, T>(f, x, out, nullptr, s);
+        const int rc = launch_segsmem<SR, T>(f, x, out, nullptr, f->nrows > 0, s);
         if (rc != GBK_SUCCESS) return rc;
         if (f->check) {  // first call on this structure: confirm no index check fired
             int32_t e = 0;
