@@ -244,8 +244,8 @@ def dominant_kernel(fmt_name, scale, graph):
         return ("k_sell_items (+ k_piece_fold for long-row pieces, k_sell_fold, k_spmv_binned for the few "
                 "problematic slices); achieved counts the whole SpMV", f"spmv_sell_c_{tag}")
     if fmt_name == "CSR_SEG":
-        return "k_segsmem (x windows staged in shared memory); achieved counts the whole SpMV", \
-            f"spmv_csr_seg_staged_{tag}"
+        return "k_segsmem (x windows staged in shared memory; + k_ss_identity for y); achieved counts the whole " \
+            "SpMV", f"spmv_csr_seg_staged_{tag}"
     if fmt_name == "CSR":
         return "k_spmv_binned (+ k_spmv_split_fixup); achieved counts the whole SpMV", f"spmv_csr_kernels_{tag}"
     return f"{fmt_name} kernels; achieved counts the whole SpMV", f"spmv_{fmt_name.lower()}_{tag}"
