@@ -40,6 +40,7 @@ CU_SOURCES = [
     "noalloc.cu",
     "batched.cu",
     "serve.cu",
+    "ingest.cu",
 ]
 
 LABLAS_SOURCES = ["lablas_capi.cpp"]

@@ -81,6 +81,13 @@ class TuneResult(C.Structure):
         return d
 
 
+class FileInfo(C.Structure):
+    _fields_ = [("nrows", C.c_int64), ("ncols", C.c_int64), ("nnz", C.c_int64), ("file_bytes", C.c_int64),
+                ("data_offset", C.c_int64), ("kind", C.c_int32), ("vtype", C.c_int32)]
+
+    KINDS = {0: "mtx", 1: "mtxbin", 2: "csr"}
+
+
 class Mask(C.Structure):
     """gbk_mask: dense (dense != NULL) or sparse (ids, nvals) mask argument."""
     _fields_ = [("dense", C.c_void_p), ("dtype", C.c_int32), ("mode", C.c_int32), ("ids", C.c_void_p),
@@ -123,6 +130,11 @@ def _declare(lib):
         "gbk_ppr": ([vp, vp, ci, C.c_double, C.c_double, ci, vp, vp, vp], ci),
         "gbk_sssp_multi": ([vp, vp, ci, vp, vp, vp], ci),
         "gbk_batch_autotune": ([vp, ci, vp, ci, C.POINTER(BatchTuneResult), vp], ci),
+        "gbk_file_info_read": ([C.c_char_p, C.POINTER(FileInfo)], ci),
+        "gbk_matrix_create_from_file": ([C.POINTER(vp), C.c_char_p, ci, vp], ci),
+        "gbk_matrix_save_csr": ([vp, C.c_char_p, vp], ci),
+        "gbk_matrix_load_csr": ([C.POINTER(vp), C.c_char_p, vp], ci),
+        "gbk_matrix_download_csr": ([vp, vp, vp, vp, vp], ci),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name, None)
@@ -156,6 +168,13 @@ def check(status: int, where: str):
 
 def init(device: int = 0):
     check(lib().gbk_init(device), "gbk_init")
+
+
+def file_info(path) -> FileInfo:
+    """Header of a .mtx / .mtxbin / .gbkcsr file."""
+    inf = FileInfo()
+    check(lib().gbk_file_info_read(str(path).encode(), C.byref(inf)), "gbk_file_info_read")
+    return inf
 
 
 def launch_count() -> int:
@@ -207,6 +226,41 @@ class Matrix:
         if val is None:
             val = np.ones(g.nnz, dtype=np.float32)
         return cls(g.row_ptr, g.col, val, stream=stream)
+
+    @classmethod
+    def _adopt(cls, h) -> "Matrix":
+        m = cls.__new__(cls)
+        m.h = h
+        inf = m.info()
+        m.n, m.ncols, m.nnz, m.vtype = int(inf.nrows), int(inf.ncols), int(inf.nnz), int(inf.vtype)
+        return m
+
+    @classmethod
+    def from_file(cls, path, dtype="f32", stream=None) -> "Matrix":
+        """Matrix from a .mtx / .mtxbin graph file (parsed on the device, every value 1) or a
+        .gbkcsr CSR cache (Matrix<T>::init_from_mtx)."""
+        h = C.c_void_p()
+        check(lib().gbk_matrix_create_from_file(C.byref(h), str(path).encode(), {"f32": F32, "i32": I32}[dtype],
+                                                stream_ptr(stream)), "gbk_matrix_create_from_file")
+        return cls._adopt(h)
+
+    @classmethod
+    def load_csr(cls, path, stream=None) -> "Matrix":
+        h = C.c_void_p()
+        check(lib().gbk_matrix_load_csr(C.byref(h), str(path).encode(), stream_ptr(stream)), "gbk_matrix_load_csr")
+        return cls._adopt(h)
+
+    def save_csr(self, path, stream=None):
+        check(lib().gbk_matrix_save_csr(self.h, str(path).encode(), stream_ptr(stream)), "gbk_matrix_save_csr")
+
+    def download_csr(self, stream=None):
+        """(row_ptr, col, val) of the CSR as host numpy arrays."""
+        rp = np.empty(self.n + 1, np.int32)
+        col = np.empty(max(self.nnz, 1), np.int32)
+        val = np.empty(max(self.nnz, 1), np.float32 if self.vtype == F32 else np.int32)
+        check(lib().gbk_matrix_download_csr(self.h, ptr(rp), ptr(col), ptr(val), stream_ptr(stream)),
+              "gbk_matrix_download_csr")
+        return rp, col[:self.nnz], val[:self.nnz]
 
     def close(self):
         if self.h:

@@ -23,9 +23,11 @@
 // checked), columns sorted ascending within each row.
 
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <cmath>
+#include <string>
 #include <vector>
 #include <algorithm>
 #include <omp.h>
@@ -301,6 +303,66 @@ int64_t gbk_gen_sources(int64_t n, const int32_t* row_ptr, int64_t count, uint64
         if (row_ptr[v + 1] > row_ptr[v]) out[got++] = (int32_t)v;
     }
     return got;
+}
+
+// Matrix Market coordinate file of an edge list in the given order (1-based
+// ids; a "%g" value column when vals != NULL), like the reference's
+// EdgeListContainer::save_as_mtx (src/helpers/graph_generation/
+// edges_container.hpp) except that the entries are not re-sorted.  Lines are
+// formatted in parallel into per-thread buffers, then written in order.
+int gbk_gen_write_mtx(const char* path, int64_t nrows, int64_t ncols, int64_t nnz, const int32_t* src,
+                      const int32_t* dst, const float* vals) {
+    FILE* fp = fopen(path, "wb");
+    if (!fp) return GBK_GEN_BAD_ARG;
+    fprintf(fp, "%%%%MatrixMarket matrix coordinate %s general\n%% written by gbk_gen_write_mtx\n%lld %lld %lld\n",
+            vals ? "real" : "pattern", (long long)nrows, (long long)ncols, (long long)nnz);
+    const int64_t block = 1 << 20;  // entries per formatting block
+    const int64_t nblocks = (nnz + block - 1) / block;
+    int rc = GBK_GEN_OK;
+    for (int64_t b0 = 0; b0 < nblocks && rc == GBK_GEN_OK; b0 += 64) {
+        const int64_t b1 = std::min<int64_t>(nblocks, b0 + 64);
+        std::vector<std::string> out(b1 - b0);
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int64_t b = b0; b < b1; b++) {
+            std::string& o = out[b - b0];
+            o.reserve(block * 24);
+            char line[96];
+            for (int64_t e = b * block; e < std::min(nnz, (b + 1) * block); e++) {
+                const int len = vals ? snprintf(line, sizeof(line), "%d %d %g\n", src[e] + 1, dst[e] + 1, (double)vals[e])
+                                     : snprintf(line, sizeof(line), "%d %d\n", src[e] + 1, dst[e] + 1);
+                o.append(line, (size_t)len);
+            }
+        }
+        for (auto& o : out)
+            if (fwrite(o.data(), 1, o.size(), fp) != o.size()) rc = GBK_GEN_BAD_ARG;
+    }
+    if (fclose(fp) != 0) rc = GBK_GEN_BAD_ARG;
+    return rc;
+}
+
+// The reference's binary edge list (.mtxbin, read by binary_read_mtx_file,
+// src/backend/matrix/read_file.hpp:377-400): int64 rows, cols, nnz, then nnz
+// int64 (src, dst) pairs, 1-based.
+int gbk_gen_write_mtxbin(const char* path, int64_t nrows, int64_t ncols, int64_t nnz, const int32_t* src,
+                         const int32_t* dst) {
+    FILE* fp = fopen(path, "wb");
+    if (!fp) return GBK_GEN_BAD_ARG;
+    int64_t h[3] = {nrows, ncols, nnz};
+    int rc = fwrite(h, sizeof(h), 1, fp) == 1 ? GBK_GEN_OK : GBK_GEN_BAD_ARG;
+    std::vector<int64_t> buf;
+    const int64_t block = 1 << 22;
+    for (int64_t e0 = 0; e0 < nnz && rc == GBK_GEN_OK; e0 += block) {
+        const int64_t e1 = std::min(nnz, e0 + block);
+        buf.resize(2 * (e1 - e0));
+#pragma omp parallel for schedule(static)
+        for (int64_t e = e0; e < e1; e++) {
+            buf[2 * (e - e0)] = (int64_t)src[e] + 1;
+            buf[2 * (e - e0) + 1] = (int64_t)dst[e] + 1;
+        }
+        if (fwrite(buf.data(), sizeof(int64_t), buf.size(), fp) != buf.size()) rc = GBK_GEN_BAD_ARG;
+    }
+    if (fclose(fp) != 0) rc = GBK_GEN_BAD_ARG;
+    return rc;
 }
 
 }  // extern "C"

@@ -115,6 +115,22 @@ int gbk_lablas_graph_create(gbk_lablas_graph* out, int64_t n, const int32_t* row
     });
 }
 
+int gbk_lablas_graph_from_file(gbk_lablas_graph* out, const char* path) {
+    if (!out || !path) return GBK_NULL_POINTER;
+    return guarded([&] {
+        auto m = std::make_unique<lablas::Matrix<float>>();
+        m->init_from_mtx(path);
+        if (m->ncols() != m->nrows()) throw "graph file: the algorithms need a square matrix (rows == cols)";
+        auto* g = new gbk_lablas_graph_s();
+        g->n = m->nrows();
+        g->rp = m->host_row_ptr();
+        g->col = m->host_col();
+        g->Af = std::move(m);
+        *out = g;
+        return 0;
+    });
+}
+
 int gbk_lablas_graph_destroy(gbk_lablas_graph g) {
     delete g;
     return 0;

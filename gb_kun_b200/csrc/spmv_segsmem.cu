@@ -226,7 +226,7 @@ __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, c
                                                int64_t qa, int64_t qb, int64_t a, int64_t b, int* next, T* out,
                                                int64_t nvrows, int64_t nrows, int32_t* err) {
     using S = Semiring<SR, T>;
-    constexpr int kRowsAhead = 3;  // runs per lane whose rows are loaded at the start of a chunk
+    constexpr int kRowsAhead = 2;  // runs per lane whose rows are loaded at the start of a chunk
     const unsigned kAll = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned le = (lane == 31) ? kAll : ((2u << lane) - 1u);
@@ -339,7 +339,7 @@ __device__ __forceinline__ void ss_warp_chunks(const uint4* __restrict__ col8, c
             if (fold && ok) fold_into<SR, T>(out, rr[k], v);
             bad_row |= fold && !ok;
         }
-        for (int j = lane + 32 * kRowsAhead; j <= nrun; j += 32) {  // chunks with 96 runs or more
+        for (int j = lane + 32 * kRowsAhead; j <= nrun; j += 32) {  // chunks with 64 runs or more
             const T v = buf[j];
             if (changes<SR, T>(v)) {
                 const uint32_t vr = (uint32_t)(cv + j);
@@ -535,7 +535,7 @@ void cut_shares(const std::vector<double>& w, int64_t nnz, int nsh, std::vector<
 // cycles), spread each share's time over its chunks by the modelled cost and
 // cut again at equal time; a few rounds settle it.  The model alone leaves
 // the slowest CTA 1.2 - 1.5x above the mean on power-law graphs.
-constexpr int kCalibrationRounds = 3;
+constexpr int kCalibrationRounds = 6;
 
 int calibrate_shares(SegSmem* f, const std::vector<double>& cost, std::vector<int32_t>& share, cudaStream_t s) {
     const int nsh = f->nshares;

@@ -39,6 +39,9 @@ def _lib():
         lib.gbk_gen_vector_f32.argtypes = [C.c_int64, C.c_uint64, C.c_void_p]
         lib.gbk_gen_sources.argtypes = [C.c_int64, C.c_void_p, C.c_int64, C.c_uint64, C.c_void_p]
         lib.gbk_gen_sources.restype = C.c_int64
+        lib.gbk_gen_write_mtx.argtypes = [C.c_char_p, C.c_int64, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
+                                          C.c_void_p]
+        lib.gbk_gen_write_mtxbin.argtypes = [C.c_char_p, C.c_int64, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]
         _LIB = lib
     return _LIB
 
@@ -125,3 +128,29 @@ def sources(g: Graph, count: int, seed: int = 45) -> np.ndarray:
     out = np.empty(count, dtype=np.int32)
     got = _lib().gbk_gen_sources(g.n, _p(g.row_ptr), count, seed, _p(out))
     return out[:got]
+
+
+def edge_list(g: Graph):
+    """(src, dst) int32 arrays of the CSR in row order."""
+    return np.repeat(np.arange(g.n, dtype=np.int32), g.degrees()), np.ascontiguousarray(g.col, dtype=np.int32)
+
+
+def write_mtx(path, nrows: int, ncols: int, src, dst, vals=None):
+    """Matrix Market coordinate file of the edge list in the given order (1-based; a value column when
+    vals is given)."""
+    s = np.ascontiguousarray(src, dtype=np.int32)
+    d = np.ascontiguousarray(dst, dtype=np.int32)
+    v = None if vals is None else np.ascontiguousarray(vals, dtype=np.float32)
+    rc = _lib().gbk_gen_write_mtx(str(path).encode(), nrows, ncols, len(s), _p(s), _p(d),
+                                  None if v is None else _p(v))
+    if rc:
+        raise RuntimeError(f"gbk_gen_write_mtx failed: {rc}")
+
+
+def write_mtxbin(path, nrows: int, ncols: int, src, dst):
+    """The reference's binary edge list: int64 rows, cols, nnz, then int64 1-based pairs."""
+    s = np.ascontiguousarray(src, dtype=np.int32)
+    d = np.ascontiguousarray(dst, dtype=np.int32)
+    rc = _lib().gbk_gen_write_mtxbin(str(path).encode(), nrows, ncols, len(s), _p(s), _p(d))
+    if rc:
+        raise RuntimeError(f"gbk_gen_write_mtxbin failed: {rc}")

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "core.hpp"
+#include "gbk_ingest.h"
 
 namespace lablas {
 
@@ -116,6 +117,29 @@ public:
         return upload(nrows, nrows);
     }
 
+    // init_from_mtx (src/cpp_graphblas/matrix.hpp:107-110 ->
+    // src/backend/matrix/read_file.hpp:565-617): a .mtx / .mtxbin file (or a
+    // .gbkcsr CSR cache) parsed on the device; rows keep the file's order and
+    // every value is 1.  Throws on a missing or malformed file.
+    void init_from_mtx(const std::string& name) {
+        release();
+        int rc = gbk_matrix_create_from_file(&h_, name.c_str(), dtype, stream());
+        throw_if(rc, "init_from_mtx");
+        gbk_matrix_info inf;
+        gbk_matrix_get_info(h_, &inf);
+        nrows_ = (Index)inf.nrows;
+        ncols_ = (Index)inf.ncols;
+        nnz_ = (Index)inf.nnz;
+        rp_.resize(nrows_ + 1);
+        col_.resize(nnz_);
+        val_.resize(nnz_);
+        rc = gbk_matrix_download_csr(h_, rp_.data(), col_.data(), val_.data(), stream());
+        throw_if(rc, "init_from_mtx");
+        rowdeg_.clear();
+        coldeg_.clear();
+        apply_format();
+    }
+
     Index* get_rowdegrees() {
         degrees();
         return rowdeg_.data();
@@ -163,7 +187,13 @@ public:
         for (Index i = 0; i < nrows_; i++) rp_[i + 1] += rp_[i];
         upload(nrows_, ncols_);
     }
-    void sort_csr_columns(const std::string&) {}  // rows are always kept column-sorted
+    // Rows built from arrays are kept column-sorted; rows read from a file keep
+    // the file's order until this sorts them (matrix.hpp:66-127).
+    void sort_csr_columns(const std::string&) {
+        if (rows_sorted()) return;
+        sort_rows();
+        upload(nrows_, ncols_);
+    }
     void sort_csc_rows(const std::string&) {}     // the device CSC is built row-sorted
     void print() const {
         for (Index i = 0; i < nrows_; i++) {
@@ -199,6 +229,11 @@ public:
     }
 
 private:
+    bool rows_sorted() const {
+        for (size_t i = 0; i + 1 < rp_.size(); i++)
+            if (!std::is_sorted(col_.begin() + rp_[i], col_.begin() + rp_[i + 1])) return false;
+        return true;
+    }
     void sort_rows() {
         for (size_t i = 0; i + 1 < rp_.size(); i++) {
             int32_t a = rp_[i], b = rp_[i + 1];

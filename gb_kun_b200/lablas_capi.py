@@ -30,6 +30,7 @@ def lib():
         vp, i64, i32, dp = C.c_void_p, C.c_int64, C.c_int32, C.POINTER(C.c_double)
         L.gbk_lablas_graph_create.argtypes = [C.POINTER(vp), i64, vp, vp, vp]
         L.gbk_lablas_graph_destroy.argtypes = [vp]
+        L.gbk_lablas_graph_from_file.argtypes = [C.POINTER(vp), C.c_char_p]
         L.gbk_lablas_get_last_error.argtypes = [C.c_char_p, C.c_size_t]
         L.gbk_lablas_bfs.argtypes = [vp, i64, vp, dp]
         L.gbk_lablas_cc.argtypes = [vp, vp, C.POINTER(i32), dp]
@@ -66,6 +67,19 @@ class Graph:
         self.h = C.c_void_p()
         rp, col, w = self._keep
         _check(lib().gbk_lablas_graph_create(C.byref(self.h), g.n, _p(rp), _p(col), _p(w)), "graph_create")
+
+    @classmethod
+    def from_file(cls, path) -> "Graph":
+        """Graph from a .mtx / .mtxbin file or a .gbkcsr cache (lablas::Matrix<float>::init_from_mtx,
+        parsed on the device; unit weights)."""
+        from . import capi
+        capi.init(0)
+        self = cls.__new__(cls)
+        self.n = int(capi.file_info(path).nrows)
+        self._keep = None
+        self.h = C.c_void_p()
+        _check(lib().gbk_lablas_graph_from_file(C.byref(self.h), str(path).encode()), "graph_from_file")
+        return self
 
     def close(self):
         if self.h:

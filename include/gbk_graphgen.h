@@ -48,6 +48,16 @@ void gbk_gen_vector_f32(int64_t n, uint64_t seed, float* out);
 /* `count` seeded vertices with non-zero out-degree; returns how many were found. */
 int64_t gbk_gen_sources(int64_t n, const int32_t* row_ptr, int64_t count, uint64_t seed, int32_t* out);
 
+/* Graph files for ingest tests and benchmarks, entries in the given order.
+ * .mtx: Matrix Market coordinate text, 1-based, "pattern" or (vals != NULL)
+ * "real" with a %g value column.  .mtxbin: int64 rows, cols, nnz, then int64
+ * 1-based (src, dst) pairs, the layout binary_read_mtx_file reads
+ * (src/backend/matrix/read_file.hpp:377-400). */
+int gbk_gen_write_mtx(const char* path, int64_t nrows, int64_t ncols, int64_t nnz, const int32_t* src,
+                      const int32_t* dst, const float* vals);
+int gbk_gen_write_mtxbin(const char* path, int64_t nrows, int64_t ncols, int64_t nnz, const int32_t* src,
+                         const int32_t* dst);
+
 #ifdef __cplusplus
 }
 #endif

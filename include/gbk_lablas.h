@@ -24,6 +24,11 @@ typedef struct gbk_lablas_graph_s* gbk_lablas_graph;
 /* weights: NULL for unit weights, else nnz int32 edge weights (SSSP). */
 int gbk_lablas_graph_create(gbk_lablas_graph* out, int64_t n, const int32_t* row_ptr, const int32_t* col,
                             const int32_t* weights);
+/* Graph from a .mtx / .mtxbin file (or a .gbkcsr CSR cache) through
+ * lablas::Matrix<float>::init_from_mtx, as the reference's drivers load a
+ * graph file (src/helpers/lib_kernels/init_matrix.h:11-14); unit weights,
+ * rows in the file's order.  The file's row and column counts must agree. */
+int gbk_lablas_graph_from_file(gbk_lablas_graph* out, const char* path);
 int gbk_lablas_graph_destroy(gbk_lablas_graph g);
 int gbk_lablas_get_last_error(char* buf, size_t len);
 

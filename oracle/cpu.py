@@ -48,7 +48,27 @@ class Oracle:
         L.orc_tc.argtypes = [i64, vp, vp]
         L.orc_tc.restype = C.c_uint64
         L.orc_transpose.argtypes = [i64, vp, vp, vp, vp, vp, vp]
+        L.orc_read_graph_file.argtypes = [C.c_char_p, C.c_int, vp, vp, vp, vp, vp, vp]
+        L.orc_read_graph_file.restype = C.c_int
         self.L = L
+
+    def read_graph_file(self, path, kind=None):
+        """(nrows, ncols, row_ptr, col) of a .mtx (kind 0) / .mtxbin (kind 1) file, rows in file order.
+        Raises ValueError(code, bad_line) on a bad file."""
+        if kind is None:
+            kind = 1 if str(path).endswith("mtxbin") else 0
+        r, c, z, bad = C.c_int64(0), C.c_int64(0), C.c_int64(0), C.c_int64(0)
+        rc = self.L.orc_read_graph_file(str(path).encode(), kind, C.byref(r), C.byref(c), C.byref(z), None, None,
+                                        None)
+        if rc:
+            raise ValueError(rc, 0)
+        rp = np.empty(r.value + 1, np.int32)
+        col = np.empty(max(z.value, 1), np.int32)
+        rc = self.L.orc_read_graph_file(str(path).encode(), kind, C.byref(r), C.byref(c), C.byref(z), _p(rp),
+                                        _p(col), C.byref(bad))
+        if rc:
+            raise ValueError(rc, bad.value)
+        return r.value, c.value, rp, col[:z.value]
 
     def spmv_f64(self, g, val, x):
         y = np.empty(g.n, dtype=np.float64)
@@ -130,6 +150,9 @@ class Reference:
             L.ref_pr.argtypes = [i64, vp, vp, C.c_int, vp, C.c_int, dp]
             L.ref_tc.argtypes = [i64, vp, vp, vp, C.c_int, dp]
             L.ref_max_threads.restype = C.c_int
+            L.ref_graph_read.argtypes = [C.c_char_p, C.POINTER(i64), C.POINTER(i64), C.POINTER(vp), dp]
+            L.ref_graph_csr.argtypes = [vp, vp, vp, vp]
+            L.ref_graph_free.argtypes = [vp]
 
     @staticmethod
     def available() -> bool:
@@ -186,3 +209,18 @@ class Reference:
         if rc:
             raise RuntimeError(f"ref_tc rc={rc}")
         return int(cnt.value), ms.value
+
+    def graph_read(self, path):
+        """The reference's Matrix<float>::init_from_mtx: (nrows, row_ptr, col, val, ms)."""
+        n, z, h, ms = C.c_int64(0), C.c_int64(0), C.c_void_p(), C.c_double(0)
+        rc = self.L.ref_graph_read(str(path).encode(), C.byref(n), C.byref(z), C.byref(h), C.byref(ms))
+        if rc:
+            raise RuntimeError(f"ref_graph_read rc={rc}")
+        try:
+            rp = np.empty(n.value + 1, np.int32)
+            col = np.empty(max(z.value, 1), np.int32)
+            val = np.empty(max(z.value, 1), np.float32)
+            self.L.ref_graph_csr(h, _p(rp), _p(col), _p(val))
+        finally:
+            self.L.ref_graph_free(h)
+        return n.value, rp, col[:z.value], val[:z.value], ms.value

@@ -11,6 +11,7 @@
 #include "oracle.h"
 
 #include <float.h>
+#include <stdio.h>
 #include <limits.h>
 #include <math.h>
 #include <stdlib.h>
@@ -439,4 +440,120 @@ void orc_transpose(int64_t n, const int32_t* rp, const int32_t* col, const float
             if (val && tval) tval[q] = val[e];
         }
     free(pos);
+}
+
+/* ------------------------------------------------------------------------ */
+/* graph files (read_file.hpp:5-22, :27-47, :52-165, :377-400, :565-617)     */
+
+static int orc_is_blank(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\n'; }
+
+/* One data line: 0 = entry (ids 1-based in *a, *b), 1 = blank or comment,
+ * 2 = malformed.  Accepts what sscanf("%lld %lld") accepts for non-negative
+ * ids followed by a blank or the end of the line. */
+static int orc_parse_line(const char* s, long long* a, long long* b) {
+    const char* p = s;
+    while (*p && orc_is_blank(*p)) p++;
+    if (!*p || *p == '%') return 1;
+    long long v[2] = {0, 0};
+    for (int f = 0; f < 2; f++) {
+        if (f) {
+            if (!(*p == ' ' || *p == '\t')) return 2;
+            while (*p == ' ' || *p == '\t') p++;
+        }
+        if (*p == '+') p++;
+        int digits = 0;
+        while (*p >= '0' && *p <= '9') {
+            v[f] = v[f] * 10 + (*p - '0');
+            if (++digits > 18) return 2;
+            p++;
+        }
+        if (!digits) return 2;
+    }
+    if (*p && !orc_is_blank(*p)) return 2;
+    *a = v[0];
+    *b = v[1];
+    return 0;
+}
+
+int orc_read_graph_file(const char* path, int kind, int64_t* nrows, int64_t* ncols, int64_t* nnz, int32_t* rp,
+                        int32_t* col, int64_t* bad_line) {
+    FILE* fp = fopen(path, kind == 0 ? "r" : "rb");
+    if (!fp) return 1;
+    long long r = 0, c = 0, z = 0;
+    char line[8192];
+    if (kind == 0) {
+        int found = 0;
+        while (fgets(line, sizeof(line), fp))
+            if (line[0] != '%') {
+                found = 1;
+                break;
+            }
+        if (!found || sscanf(line, "%lld %lld %lld", &r, &c, &z) != 3 || r < 0 || c < 0 || z < 0) {
+            fclose(fp);
+            return 2;
+        }
+    } else {
+        int64_t h[3];
+        if (fread(h, sizeof(h), 1, fp) != 1 || h[0] < 0 || h[1] < 0 || h[2] < 0) {
+            fclose(fp);
+            return 2;
+        }
+        r = h[0];
+        c = h[1];
+        z = h[2];
+    }
+    *nrows = r;
+    *ncols = c;
+    *nnz = z;
+    if (!rp) {
+        fclose(fp);
+        return 0;
+    }
+    int32_t* src = (int32_t*)malloc(sizeof(int32_t) * (size_t)(z > 0 ? z : 1));
+    int32_t* dst = (int32_t*)malloc(sizeof(int32_t) * (size_t)(z > 0 ? z : 1));
+    int rc = 0;
+    int64_t got = 0, ln = 0;
+    while (got < z) {
+        long long a = 0, b = 0;
+        if (kind == 0) {
+            if (!fgets(line, sizeof(line), fp)) break;
+            ln++;
+            const int t = orc_parse_line(line, &a, &b);
+            if (t == 1) continue;
+            if (t == 2 || a < 1 || a > r || b < 1 || b > c) {
+                rc = 3;
+                if (bad_line) *bad_line = ln;
+                break;
+            }
+        } else {
+            int64_t pr[2];
+            if (fread(pr, sizeof(pr), 1, fp) != 1) break;
+            ln++;
+            a = pr[0];
+            b = pr[1];
+            if (a < 1 || a > r || b < 1 || b > c) {
+                rc = 3;
+                if (bad_line) *bad_line = ln;
+                break;
+            }
+        }
+        src[got] = (int32_t)(a - 1);
+        dst[got] = (int32_t)(b - 1);
+        got++;
+    }
+    fclose(fp);
+    if (rc == 0 && got < z) rc = 4;
+    if (rc == 0) {
+        /* counting sort by row: a row keeps the file order */
+        for (int64_t i = 0; i <= r; i++) rp[i] = 0;
+        for (int64_t e = 0; e < z; e++) rp[src[e] + 1]++;
+        for (int64_t i = 0; i < r; i++) rp[i + 1] += rp[i];
+        int32_t* fillp = (int32_t*)malloc(sizeof(int32_t) * (size_t)(r > 0 ? r : 1));
+        for (int64_t i = 0; i < r; i++) fillp[i] = rp[i];
+        for (int64_t e = 0; e < z; e++) col[fillp[src[e]]++] = dst[e];
+        free(fillp);
+    }
+    free(src);
+    free(dst);
+    return rc;
 }

@@ -74,6 +74,21 @@ uint64_t orc_tc(int64_t n, const int32_t* rp, const int32_t* col);
 void orc_transpose(int64_t n, const int32_t* rp, const int32_t* col, const float* val, int32_t* cp,
                    int32_t* row, float* tval);
 
+/* Graph file reader restating Matrix<T>::init_from_mtx
+ * (src/backend/matrix/read_file.hpp:565-617): kind 0 = .mtx text (lines
+ * starting with '%' skipped, then "rows cols nnz", then nnz lines of 1-based
+ * "row col [value]" read with fgets + sscanf as read_portion does,
+ * :5-22; rows keep the file order, as process_portion's push_back gives,
+ * :27-47), kind 1 = .mtxbin (int64 rows, cols, nnz, then int64 pairs,
+ * :377-400; rows in file order, where the reference's order follows its
+ * hash maps).  Blank and '%' lines between entries are skipped.
+ * rp == NULL: header only.  Otherwise rp (rows + 1) and col (nnz) are
+ * filled.  Returns 0, or 1 = cannot open, 2 = bad header, 3 = malformed
+ * line or id out of range (*bad_line = its data-line number, 1-based),
+ * 4 = fewer than nnz entries. */
+int orc_read_graph_file(const char* path, int kind, int64_t* nrows, int64_t* ncols, int64_t* nnz, int32_t* rp,
+                        int32_t* col, int64_t* bad_line);
+
 #ifdef __cplusplus
 }
 #endif

@@ -234,4 +234,49 @@ int ref_tc(int64_t n, const int32_t* rp, const int32_t* col, uint64_t* count, in
     }
 }
 
+// Graph file through the reference's own reader: lablas::Matrix<T>::
+// init_from_mtx (src/cpp_graphblas/matrix.hpp:107-110 -> read_file.hpp:565-617)
+// in the CSR storage format.  The matrix stays alive behind *handle until
+// ref_graph_free; ref_graph_csr copies its CSR out (int32).  At least four
+// OpenMP threads are used for .mtxbin (binary_read_mtx_file runs
+// omp_get_max_threads() / 4 threads, read_file.hpp:428).
+int ref_graph_read(const char* path, int64_t* nrows, int64_t* nnz, void** handle, double* ms) {
+    try {
+        Quiet q;
+        const int before = omp_get_max_threads();
+        if (before < 4) omp_set_num_threads(4);
+        auto* A = new lablas::Matrix<float>();
+        A->get_matrix()->set_preferred_matrix_format(CSR);
+        const double t0 = now_ms();
+        A->init_from_mtx(path);
+        if (ms) *ms = now_ms() - t0;
+        omp_set_num_threads(before);
+        const lablas::backend::MatrixCSR<float>* csr = A->get_matrix()->get_csr();
+        *nrows = (int64_t)A->get_matrix()->get_nrows();
+        *nnz = (int64_t)csr->get_nnz();
+        *handle = A;
+        return 0;
+    } catch (const char* e) {
+        std::cerr << "reference error: " << e << std::endl;
+        return 13;
+    }
+}
+
+int ref_graph_csr(void* handle, int32_t* rp, int32_t* col, float* val) {
+    auto* A = (lablas::Matrix<float>*)handle;
+    const lablas::backend::MatrixCSR<float>* csr = A->get_matrix()->get_csr();
+    const int64_t n = (int64_t)A->get_matrix()->get_nrows(), nnz = (int64_t)csr->get_nnz();
+    const ENT* p = csr->get_row_ptr();
+    const VNT* c = csr->get_col_ids();
+    const float* v = csr->get_vals();
+    for (int64_t i = 0; i <= n; i++) rp[i] = (int32_t)p[i];
+    for (int64_t e = 0; e < nnz; e++) {
+        col[e] = (int32_t)c[e];
+        if (val) val[e] = v[e];
+    }
+    return 0;
+}
+
+void ref_graph_free(void* handle) { delete (lablas::Matrix<float>*)handle; }
+
 }  // extern "C"

@@ -15,6 +15,7 @@ HEADERS = {
     "gbk_graphgen.h": ROOT / "gb_kun_b200" / "libgbk_graphgen.so",
     "gbk_lablas.h": ROOT / "gb_kun_b200" / "libgbk_lablas.so",
     "gbk_serve.h": ROOT / "gb_kun_b200" / "libgbk.so",
+    "gbk_ingest.h": ROOT / "gb_kun_b200" / "libgbk.so",
 }
 
 DECL = re.compile(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\**\s+\**(gbk_[a-z0-9_]+)\s*\(", re.M)
