@@ -65,15 +65,17 @@ def parse():
     p.add_argument("--seed", type=int, default=42)
     p.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--mode", default="spmv", choices=["spmv", "batched", "serve", "algorithms"],
+    p.add_argument("--mode", default="spmv", choices=["spmv", "batched", "serve", "algorithms", "ingest"],
                    help="spmv: the SpMV line (default); batched: 64-source BFS + 32-column PPR / SSSP on "
                         "R-MAT s22; serve: Poisson request stream on a resident undirected R-MAT s24; "
-                        "algorithms: BFS/CC/PR/SSSP/TC on undirected R-MAT s23 vs the reference CPU code")
+                        "algorithms: BFS/CC/PR/SSSP/TC on undirected R-MAT s23 vs the reference CPU code; "
+                        "ingest: the R-MAT graph as .mtx / .mtxbin files into device CSR vs the reference reader")
     p.add_argument("--queries", type=int, default=1000, help="serve: requests in the trace")
     p.add_argument("--rate", type=float, default=2000.0, help="serve: mean arrival rate (queries/s)")
     p.add_argument("--serial-queries", type=int, default=60, help="serve: requests run one at a time")
     p.add_argument("--serve-scale", type=int, default=24, help="serve: R-MAT scale of the resident graph")
     p.add_argument("--alg-scale", type=int, default=23, help="algorithms: R-MAT scale")
+    p.add_argument("--ingest-reps", type=int, default=3, help="ingest: timed reads per file")
     p.add_argument("--no-extras", action="store_true",
                    help="default line without the batched / served summaries (SpMV only)")
     return p.parse_args()
@@ -740,6 +742,101 @@ def run_algorithms(args):
     return out
 
 
+def run_ingest(args):
+    """Graph file -> device CSR (lablas::Matrix<T>::init_from_mtx, read_file.hpp:565-617) for the R-MAT
+    graph written as .mtx text and as .mtxbin, the CSR cache reload, and the reference's own reader on the
+    same files.  Files sit in a temporary directory on the local disk and are read warm (page cache): the
+    first read of each is untimed, then the median of --ingest-reps timed reads."""
+    import shutil
+    import tempfile
+    import torch
+    from gb_kun_b200 import capi, graphgen as gg
+    capi.init(0)
+    g = gg.rmat(args.scale, args.edge_factor, seed=args.seed)
+    s, d = gg.edge_list(g)
+    tmp = Path(tempfile.mkdtemp(prefix="gbk_ingest_"))
+    try:
+        f_mtx, f_bin, f_csr = tmp / "g.mtx", tmp / "g.mtxbin", tmp / "g.gbkcsr"
+        gg.write_mtx(f_mtx, g.n, g.n, s, d)
+        gg.write_mtxbin(f_bin, g.n, g.n, s, d)
+
+        def timed(path):
+            ts, A = [], None
+            for i in range(args.ingest_reps + 1):
+                if A is not None:
+                    A.close()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                A = capi.Matrix.from_file(path)
+                torch.cuda.synchronize()
+                ts.append(time.perf_counter() - t0)
+            return A, statistics.median(ts[1:])
+
+        def same(A):
+            rp, col, val = A.download_csr()
+            return bool(np.array_equal(rp, g.row_ptr) and np.array_equal(col, g.col) and np.all(val == 1))
+
+        A, t_mtx = timed(f_mtx)
+        ok_mtx = same(A)
+        A.save_csr(f_csr)
+        A.close()
+        B, t_bin = timed(f_bin)
+        ok_bin = same(B)
+        B.close()
+        Cm, t_csr = timed(f_csr)
+        Cm.close()
+        sizes = {k: os.path.getsize(f) for k, f in (("mtx", f_mtx), ("mtxbin", f_bin), ("gbkcsr", f_csr))}
+        # the link every file byte crosses once: pinned host -> device copy bandwidth
+        hb = torch.empty(1 << 30, dtype=torch.uint8).pin_memory()
+        db = torch.empty(1 << 30, dtype=torch.uint8, device="cuda")
+        db.copy_(hb, non_blocking=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            db.copy_(hb, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        h2d_gbs = 5 * (1 << 30) / (e0.elapsed_time(e1) * 1e-3) / 1e9
+        del hb, db
+        R = _ref_threads()
+        ref = {}
+        if R is not None:
+            for kind, f in (("mtx", f_mtx), ("mtxbin", f_bin)):
+                n, rp, col, val, ms = R.graph_read(f)
+                rows_equal = bool(np.array_equal(rp, g.row_ptr))
+                ref[kind] = {"ms": round(ms, 1), "MB_per_s": round(sizes[kind] / (ms * 1e-3) / 1e6, 1),
+                             "same_csr_as_ours": rows_equal and bool(np.array_equal(col, g.col)) if kind == "mtx"
+                             else rows_equal}
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    mbs = sizes["mtx"] / t_mtx / 1e6
+    out = {
+        "metric": "graph file ingest: .mtx text into device CSR (MB of file per second)", "value": round(mbs, 1),
+        "unit": "MB/s", "n_gpus": 1, "steps": args.ingest_reps, "warmup": 1, "ms_per_step": round(t_mtx * 1e3, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32 ids",
+        "data": "synthetic (seeded R-MAT written as .mtx / .mtxbin in a temporary directory)",
+        "config": {"workload": f"ingest_rmat{args.scale}", "n": g.n, "nnz": g.nnz, "file_bytes": sizes,
+                   "timing": "host timer around gbk_matrix_create_from_file (device synchronised), warm page "
+                             "cache, median of --ingest-reps after one untimed read"},
+        "mtx": {"ms": round(t_mtx * 1e3, 2), "MB_per_s": round(mbs, 1),
+                "M_entries_per_s": round(g.nnz / t_mtx / 1e6, 1), "bit_exact": ok_mtx},
+        "mtxbin": {"ms": round(t_bin * 1e3, 2), "MB_per_s": round(sizes["mtxbin"] / t_bin / 1e6, 1),
+                   "bit_exact": ok_bin},
+        "csr_cache": {"ms": round(t_csr * 1e3, 2), "MB_per_s": round(sizes["gbkcsr"] / t_csr / 1e6, 1)},
+        "roofline": {"bound": "host-to-device link (every file byte crosses it once)", "achieved": round(mbs / 1e3, 2),
+                     "peak": round(h2d_gbs, 2), "unit": "GB/s", "frac": round(mbs / 1e3 / h2d_gbs, 3),
+                     "peak_source": "measured here: pinned 1 GiB host-to-device copies"},
+        "reference": ref,
+        "cpu_baseline": None if not ref else {
+            "value": ref["mtx"]["MB_per_s"], "unit": "MB/s", "cores": R.max_threads(), "kind": "reference",
+            "sample": "one init_from_mtx of the same .mtx file (read_mtx_file_pipelined + CSR/CSC build)"},
+    }
+    if ref:
+        out["speedup_vs_reference"] = {k: round(ref[k]["ms"] / (1e3 * (t_mtx if k == "mtx" else t_bin)), 1)
+                                       for k in ref}
+    return out
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -773,7 +870,8 @@ def run_reference(args):
 def main():
     args = parse()
     if args.mode != "spmv":
-        out = {"batched": run_batched, "serve": run_serve, "algorithms": run_algorithms}[args.mode](args)
+        out = {"batched": run_batched, "serve": run_serve, "algorithms": run_algorithms,
+               "ingest": run_ingest}[args.mode](args)
         print(json.dumps(out), flush=True)
     elif args.impl == "reference":
         run_reference(args)

@@ -9,7 +9,7 @@
 // CSR is then copied out of the vectors (vector_of_vectors_to_csr,
 // src/helpers/lib_kernels/format_conversions.h:27-49).
 //
-// Here the host only moves bytes: the file is read in 64 MiB pieces by
+// Here the host only moves bytes: the file is read in 8 MiB pieces by
 // several pread threads into pinned buffers (two, so reading the next piece
 // overlaps the device work on this one), each piece is cut at its last
 // newline and copied to the device, and the device
@@ -43,7 +43,7 @@
 namespace gbk {
 namespace {
 
-constexpr int64_t kPieceBytesDefault = 64ll << 20;  // file bytes per read / parse step
+constexpr int64_t kPieceBytesDefault = 8ll << 20;  // file bytes per read / parse step
 
 // GBK_INGEST_PIECE_BYTES (at least 64) overrides the piece size, so small
 // files can exercise the piece boundaries.
@@ -52,7 +52,14 @@ int64_t piece_bytes() {
     const long long v = e ? atoll(e) : 0;
     return v >= 64 ? (int64_t)v : kPieceBytesDefault;
 }
-constexpr int kReadThreads = 4;
+constexpr int kReadThreadsDefault = 8;
+
+// GBK_INGEST_READ_THREADS overrides the pread threads per piece (1 .. 64).
+int read_threads() {
+    const char* e = getenv("GBK_INGEST_READ_THREADS");
+    const int v = e ? atoi(e) : 0;
+    return v >= 1 && v <= 64 ? v : kReadThreadsDefault;
+}
 constexpr char kCsrMagic[8] = {'G', 'B', 'K', 'C', 'S', 'R', '0', '1'};
 constexpr int64_t kCsrHeaderBytes = 64;
 
@@ -77,11 +84,11 @@ struct Fd {  // a file descriptor closed on scope exit
     }
 };
 
-// Read len bytes at offset off into dst with kReadThreads pread threads;
+// Read len bytes at offset off into dst with read_threads() pread threads;
 // returns the bytes read (short only at the end of the file) or -1.
 int64_t read_at(int fd, char* dst, int64_t off, int64_t len) {
     if (len <= 0) return 0;
-    const int nt = len >= (4ll << 20) ? kReadThreads : 1;
+    const int nt = len >= (4ll << 20) ? read_threads() : 1;
     std::vector<int64_t> got(nt, 0);
     auto work = [&](int t) {
         const int64_t a = len * t / nt, b = len * (t + 1) / nt;
@@ -165,14 +172,15 @@ __global__ void k_parse_lines(const char* __restrict__ t, const int32_t* __restr
     keep[k] = 1;
 }
 
-// .mtxbin pairs (int64, 1-based) -> 0-based int32; *bad = first pair out of range.
-__global__ void k_bin_pairs(const int64_t* __restrict__ p, int64_t npairs, int64_t nrows, int64_t ncols,
-                            int32_t* __restrict__ src, int32_t* __restrict__ dst, int64_t* bad) {
+// .mtxbin pairs (int64, 1-based) -> 0-based int32; *bad = the first pair out
+// of range, numbered from the start of the file (first = this piece's start).
+__global__ void k_bin_pairs(const int64_t* __restrict__ p, int64_t npairs, int64_t first, int64_t nrows,
+                            int64_t ncols, int32_t* __restrict__ src, int32_t* __restrict__ dst, int64_t* bad) {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= npairs) return;
     const int64_t a = p[2 * k], b = p[2 * k + 1];
     if (a < 1 || a > nrows || b < 1 || b > ncols) {
-        atomicMin((unsigned long long*)bad, (unsigned long long)k);
+        atomicMin((unsigned long long*)bad, (unsigned long long)(first + k));
         src[k] = 0;
         dst[k] = 0;
         return;
@@ -553,40 +561,48 @@ int read_mtxbin(gbk_matrix* out, const char* path, const gbk_file_info& info, gb
         GBK_CUDA(cudaMalloc(&P.text[b], kPieceBytes));
         GBK_CUDA(cudaEventCreateWithFlags(&P.copied[b], cudaEventDisableTiming));
     }
-    int64_t done = 0;
+    // pieces go out back to back: a buffer is refilled once its copy is done,
+    // and the id check is read once at the end
     int cur = 0;
-    auto fill = [&](int b, int64_t first) -> int64_t {
-        const int64_t k = std::min<int64_t>(pairs_per_piece, nnz - first);
-        const int64_t got = read_at(f.fd, P.host[b], info.data_offset + 16 * first, 16 * k);
-        return got == 16 * k ? k : -1;
-    };
-    int64_t k = nnz > 0 ? fill(cur, 0) : 0;
-    GBK_REQUIRE(k >= 0, GBK_INVALID_VALUE, "%s: read error", path);
-    while (done < nnz) {
+    for (int64_t done = 0; done < nnz; done += pairs_per_piece, cur ^= 1) {
+        const int64_t k = std::min<int64_t>(pairs_per_piece, nnz - done);
+        GBK_CUDA(cudaEventSynchronize(P.copied[cur]));
+        GBK_REQUIRE(read_at(f.fd, P.host[cur], info.data_offset + 16 * done, 16 * k) == 16 * k, GBK_INVALID_VALUE,
+                    "%s: read error", path);
         GBK_CUDA(cudaMemcpyAsync(P.text[cur], P.host[cur], 16 * k, cudaMemcpyHostToDevice, s));
         GBK_CUDA(cudaEventRecord(P.copied[cur], s));
-        k_bin_pairs<<<nblocks(k), 256, 0, s>>>((const int64_t*)P.text[cur], k, info.nrows, info.ncols,
+        k_bin_pairs<<<nblocks(k), 256, 0, s>>>((const int64_t*)P.text[cur], k, done, info.nrows, info.ncols,
                                                 coo_src + done, coo_dst + done, bad);
         GBK_LAUNCHED();
-        // (k_bin_pairs reports the piece-local index; the piece's start is added on the host)
-        int64_t b = 0;
-        GBK_CUDA(cudaMemcpyAsync(&b, bad, 8, cudaMemcpyDeviceToHost, s));
-        const int nxt = cur ^ 1;
-        int64_t nk = 0;
-        if (done + k < nnz) {
-            GBK_CUDA(cudaEventSynchronize(P.copied[nxt]));
-            nk = fill(nxt, done + k);
-            GBK_REQUIRE(nk >= 0, GBK_INVALID_VALUE, "%s: read error", path);
-        }
-        GBK_CUDA(cudaStreamSynchronize(s));
-        GBK_REQUIRE(b == 0x7f7f7f7f7f7f7f7fll, GBK_INVALID_VALUE,
-                    "%s: entry %lld has an id outside 1..%lld / 1..%lld", path, (long long)(done + b + 1),
-                    (long long)info.nrows, (long long)info.ncols);
-        done += k;
-        k = nk;
-        cur = nxt;
     }
+    int64_t first_bad = 0;
+    GBK_CUDA(cudaMemcpyAsync(&first_bad, bad, 8, cudaMemcpyDeviceToHost, s));
+    GBK_CUDA(cudaStreamSynchronize(s));
+    GBK_REQUIRE(first_bad == 0x7f7f7f7f7f7f7f7fll, GBK_INVALID_VALUE,
+                "%s: entry %lld has an id outside 1..%lld / 1..%lld", path, (long long)(first_bad + 1),
+                (long long)info.nrows, (long long)info.ncols);
     return coo_to_matrix(out, info.nrows, info.ncols, nnz, coo_src, coo_dst, vtype, s);
+}
+
+// Copy file bytes [off, off + bytes) to device memory dst through the two
+// pinned piece buffers (the read of one piece overlaps the copy of the other).
+int stream_to_device(int fd, const char* path, int64_t off, int64_t bytes, char* dst, cudaStream_t s) {
+    const int64_t piece = std::max<int64_t>(16, piece_bytes());
+    Pieces P;
+    for (int b = 0; b < 2; ++b) {
+        GBK_CUDA(cudaHostAlloc(&P.host[b], std::min(piece, std::max<int64_t>(bytes, 1)), cudaHostAllocDefault));
+        GBK_CUDA(cudaEventCreateWithFlags(&P.copied[b], cudaEventDisableTiming));
+    }
+    int cur = 0;
+    for (int64_t done = 0; done < bytes; done += piece, cur ^= 1) {
+        const int64_t k = std::min(piece, bytes - done);
+        GBK_CUDA(cudaEventSynchronize(P.copied[cur]));  // the copy that last used this buffer is done
+        GBK_REQUIRE(read_at(fd, P.host[cur], off + done, k) == k, GBK_INVALID_VALUE, "%s: read error", path);
+        GBK_CUDA(cudaMemcpyAsync(dst + done, P.host[cur], k, cudaMemcpyHostToDevice, s));
+        GBK_CUDA(cudaEventRecord(P.copied[cur], s));
+    }
+    GBK_CUDA(cudaStreamSynchronize(s));
+    return GBK_SUCCESS;
 }
 
 int load_csr(gbk_matrix* out, const char* path, const gbk_file_info& info, cudaStream_t s) {
@@ -598,41 +614,33 @@ int load_csr(gbk_matrix* out, const char* path, const gbk_file_info& info, cudaS
     Fd f;
     f.fd = open(path, O_RDONLY);
     GBK_REQUIRE(f.fd >= 0, GBK_INVALID_VALUE, "can not open CSR cache %s", path);
-    char* h = nullptr;
-    GBK_CUDA(cudaHostAlloc(&h, std::max<int64_t>(bytes, 16), cudaHostAllocDefault));
-    struct HostFree {
-        char* p;
-        ~HostFree() { cudaFreeHost(p); }
-    } hf{h};
-    GBK_REQUIRE(read_at(f.fd, h, kCsrHeaderBytes, bytes) == bytes, GBK_INVALID_VALUE, "%s: read error", path);
-    const int32_t* ptr = (const int32_t*)h;
+    char* d = nullptr;  // row pointers, column ids and values back to back, as in the file
+    int32_t* bad = nullptr;
+    struct DevFree {
+        char** a;
+        int32_t** b;
+        ~DevFree() {
+            cudaFree(*a);
+            cudaFree(*b);
+        }
+    } df{&d, &bad};
+    GBK_CUDA(cudaMalloc(&d, std::max<int64_t>(bytes, 16)));
+    GBK_CUDA(cudaMalloc(&bad, 4));
+    int rc = stream_to_device(f.fd, path, kCsrHeaderBytes, bytes, d, s);
+    if (rc) return rc;
+    const int32_t* ptr = (const int32_t*)d;
     const int32_t* col = ptr + n + 1;
     const void* val = col + nnz;
-    gbk_matrix A = nullptr;
-    int rc = gbk_matrix_create_csr(&A, n, info.ncols, nnz, ptr, col, val, (gbk_dtype)info.vtype, 0, s);
-    if (rc) return rc;
     // a cache is input: check it before any kernel indexes with it
-    const int32_t *dptr = nullptr, *dcol = nullptr;
-    gbk_matrix_csr_arrays(A, 0, &dptr, &dcol, nullptr, s);
-    int32_t* bad = nullptr;
     int32_t hb = 0;
-    cudaError_t e = cudaMalloc(&bad, 4);
-    if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, 4, s);
-    if (e == cudaSuccess) {
-        k_check_csr<<<nblocks(std::max(n + 1, nnz)), 256, 0, s>>>(dptr, dcol, n, info.ncols, nnz, bad);
-        count_launch(1);
-        e = cudaMemcpyAsync(&hb, bad, 4, cudaMemcpyDeviceToHost, s);
-    }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(bad);
-    if (e != cudaSuccess || hb != 0) {
-        gbk_matrix_destroy(A);
-        if (e != cudaSuccess) return cuda_fail(e, "CSR cache check", __FILE__, __LINE__);
-        set_error("%s: corrupt CSR cache (%s)", path, hb == 1 ? "row pointers" : "column ids");
-        return GBK_INVALID_VALUE;
-    }
-    *out = A;
-    return GBK_SUCCESS;
+    GBK_CUDA(cudaMemsetAsync(bad, 0, 4, s));
+    k_check_csr<<<nblocks(std::max(n + 1, nnz)), 256, 0, s>>>(ptr, col, n, info.ncols, nnz, bad);
+    GBK_LAUNCHED();
+    GBK_CUDA(cudaMemcpyAsync(&hb, bad, 4, cudaMemcpyDeviceToHost, s));
+    GBK_CUDA(cudaStreamSynchronize(s));
+    GBK_REQUIRE(hb == 0, GBK_INVALID_VALUE, "%s: corrupt CSR cache (%s)", path,
+                hb == 1 ? "row pointers" : "column ids");
+    return gbk_matrix_create_csr(out, n, info.ncols, nnz, ptr, col, val, (gbk_dtype)info.vtype, 1, s);
 }
 
 }  // namespace
