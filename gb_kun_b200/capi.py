@@ -27,6 +27,8 @@ BINOP = {"second": 0, "first": 1, "plus": 2, "minus": 3, "times": 4, "div": 5, "
 UNOP = {"identity": 0, "abs": 1, "one": 2}
 MASK = {"scmp": 0, "comp": 2, "structure": 4, "str_comp": 5, "default": 6}
 MONOID = {"plus": 0, "min": 1, "max": 2, "lor": 3, "land": 4, "times": 5}
+SELECT = {"tril": 0, "triu": 1, "diag": 2, "offdiag": 3, "value_eq": 4, "value_ne": 5, "value_gt": 6,
+          "value_ge": 7, "value_lt": 8, "value_le": 9}
 
 
 class GbkError(RuntimeError):
@@ -130,6 +132,9 @@ def _declare(lib):
         "gbk_ppr": ([vp, vp, ci, C.c_double, C.c_double, ci, vp, vp, vp], ci),
         "gbk_sssp_multi": ([vp, vp, ci, vp, vp, vp], ci),
         "gbk_batch_autotune": ([vp, ci, vp, ci, C.POINTER(BatchTuneResult), vp], ci),
+        "gbk_mxm": ([C.POINTER(vp), vp, vp, ci, vp], ci),
+        "gbk_select_matrix": ([C.POINTER(vp), vp, ci, C.c_double, vp], ci),
+        "gbk_select_vector": ([ci, C.c_double, vp, ci, vp, ci, i64, ci, mp, ci, vp], ci),
         "gbk_file_info_read": ([C.c_char_p, C.POINTER(FileInfo)], ci),
         "gbk_matrix_create_from_file": ([C.POINTER(vp), C.c_char_p, ci, vp], ci),
         "gbk_matrix_save_csr": ([vp, C.c_char_p, vp], ci),
@@ -168,6 +173,18 @@ def check(status: int, where: str):
 
 def init(device: int = 0):
     check(lib().gbk_init(device), "gbk_init")
+
+
+def select_vector(w, u, op: str, thunk=0.0, accum="second", mask=None, mask_mode="default", replace=False,
+                  stream=None):
+    """w[i] = accum(w[i], u[i] if op keeps (u[i], i) else 0) where the dense mask selects (all i without one)."""
+    m = None
+    if mask is not None:
+        m = Mask(ptr(mask), dtype_code(mask), MASK[mask_mode], None, 0)
+    check(lib().gbk_select_vector(SELECT[op], float(thunk), ptr(w), dtype_code(w), ptr(u), dtype_code(u),
+                                  int(w.numel()), BINOP[accum], None if m is None else C.byref(m), int(replace),
+                                  stream_ptr(stream)), "gbk_select_vector")
+    return w
 
 
 def file_info(path) -> FileInfo:
@@ -252,6 +269,19 @@ class Matrix:
 
     def save_csr(self, path, stream=None):
         check(lib().gbk_matrix_save_csr(self.h, str(path).encode(), stream_ptr(stream)), "gbk_matrix_save_csr")
+
+    def mxm(self, B: "Matrix", semiring="plus_times", stream=None) -> "Matrix":
+        """Unmasked C = self (+.x) B (SpMSpM_unmasked_ikj); zero sums dropped, rows column-sorted."""
+        h = C.c_void_p()
+        check(lib().gbk_mxm(C.byref(h), self.h, B.h, SEMIRING[semiring], stream_ptr(stream)), "gbk_mxm")
+        return Matrix._adopt(h)
+
+    def select(self, op: str, thunk=0.0, stream=None) -> "Matrix":
+        """Matrix select (select.h:363-395): same structure, values kept where op keeps them, else 0."""
+        h = C.c_void_p()
+        check(lib().gbk_select_matrix(C.byref(h), self.h, SELECT[op], float(thunk), stream_ptr(stream)),
+              "gbk_select_matrix")
+        return Matrix._adopt(h)
 
     def download_csr(self, stream=None):
         """(row_ptr, col, val) of the CSR as host numpy arrays."""

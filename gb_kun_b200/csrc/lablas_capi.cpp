@@ -228,6 +228,18 @@ int gbk_lablas_ppr(gbk_lablas_graph g, int64_t seed, int32_t itermax, double dam
     });
 }
 
+int gbk_lablas_tc_method(gbk_lablas_graph g, int32_t method, uint64_t* count, double* ms) {
+    if (!g || !count) return GBK_NULL_POINTER;
+    if (method < 0 || method > 6) return GBK_INVALID_VALUE;
+    return guarded([&] {
+        auto* A = g->unit_i();
+        Timer t(ms);
+        *count = lablas::algorithm::triangle_count(A, method);
+        t.stop();
+        return 0;
+    });
+}
+
 int gbk_lablas_tc(gbk_lablas_graph g, uint64_t* count, double* ms) {
     if (!g || !count) return GBK_NULL_POINTER;
     return guarded([&] {

@@ -7,6 +7,20 @@
 // entries and, entry by entry, its lanes split the shorter list and binary
 // search each element in the longer one, so a hub pair is spread over the
 // warp and light pairs cost a few instructions each.
+//
+// Unmasked SpGEMM C = A (+.x) B replaces SpMSpM_unmasked_ikj
+// (src/backend/spmspm/spmspm_hash_based_gustavson.h:9-148, a hash map per
+// row of C) by expand-sort-compress in row blocks: every product
+// A_ik * B_kj is written with its (i, j) key (one thread per product, found
+// by binary search over the per-entry product offsets), the block is radix
+// sorted by key, equal keys are reduced with the semiring's add, and sums
+// equal to 0 are dropped as the reference keeps only val != 0.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstdlib>
+#include <vector>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -78,11 +92,318 @@ __global__ void k_masked_spgemm(const int32_t* __restrict__ mptr, const int32_t*
     }
 }
 
+// ---------------------------------------------------------------------------
+// unmasked SpGEMM
+
+// products of A's entry e: the degree of row aidx[e] of B
+__global__ void k_entry_products(const int32_t* __restrict__ aidx, int64_t nnz, const int32_t* __restrict__ bptr,
+                                 int64_t* __restrict__ cnt) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < nnz) cnt[e] = bptr[aidx[e] + 1] - bptr[aidx[e]];
+}
+
+// product offset of each row's first entry
+__global__ void k_row_offsets(const int32_t* __restrict__ aptr, int64_t nrows, const int64_t* __restrict__ off,
+                              int64_t* __restrict__ roff) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r <= nrows) roff[r] = off[aptr[r]];
+}
+
+// row of A's entry e
+__global__ void k_entry_rows(const int32_t* __restrict__ aptr, int64_t nrows, int64_t nnz, int32_t* __restrict__ arow) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    int64_t lo = 0, hi = nrows;  // last row starting at or before e
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (aptr[mid] <= e)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    arow[e] = (int32_t)lo;
+}
+
+// Products [p0, p1) of the entries [e0, e1) (off: exclusive product offsets
+// per entry, off[e1] = p1): key (row << 32 | column), value mul(a, b).
+template <int SR, typename T>
+__global__ void k_expand(const int64_t* __restrict__ off, int64_t e0, int64_t e1, int64_t p0, int64_t p1,
+                         const int32_t* __restrict__ arow, const int32_t* __restrict__ aidx, const T* __restrict__ aval,
+                         const int32_t* __restrict__ bptr, const int32_t* __restrict__ bidx,
+                         const T* __restrict__ bval, unsigned long long* __restrict__ key, T* __restrict__ val) {
+    using S = Semiring<SR, T>;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < p1; p += stride) {
+        int64_t lo = e0, hi = e1;  // last entry whose products start at or before p
+        while (hi - lo > 1) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (off[mid] <= p)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const int32_t k = aidx[lo];
+        const int64_t f = bptr[k] + (p - off[lo]);
+        key[p - p0] = ((unsigned long long)(uint32_t)arow[lo] << 32) | (unsigned long long)(uint32_t)bidx[f];
+        val[p - p0] = S::mul(aval[lo], bval[f]);
+    }
+}
+
+template <int SR, typename T>
+struct SemiringAdd {
+    __device__ __forceinline__ T operator()(const T& a, const T& b) const { return Semiring<SR, T>::add(a, b); }
+};
+
+template <typename T>
+struct NonZero {
+    __device__ __forceinline__ bool operator()(const T& v) const { return v != T(0); }
+};
+
+__global__ void k_split_keys(const unsigned long long* __restrict__ key, int64_t n, int32_t* __restrict__ row,
+                             int32_t* __restrict__ col) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    row[i] = (int32_t)(key[i] >> 32);
+    col[i] = (int32_t)(key[i] & 0xffffffffu);
+}
+
+// ptr[r] = first entry of row >= r (rows ascending)
+__global__ void k_bounds(const int32_t* __restrict__ row, int64_t nnz, int64_t nrows, int32_t* __restrict__ ptr) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > nnz) return;
+    const int64_t lo = i == 0 ? 0 : (int64_t)row[i - 1] + 1;
+    const int64_t hi = i == nnz ? nrows : (int64_t)row[i];
+    for (int64_t r = lo; r <= hi; ++r) ptr[r] = (int32_t)i;
+}
+
+template <typename T>
+__global__ void k_nonzero_flags(const T* __restrict__ v, int64_t n, uint8_t* __restrict__ flag) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flag[i] = v[i] != T(0);
+}
+
+unsigned nb(int64_t n) { return (unsigned)std::max<int64_t>(1, (n + 255) / 256); }
+
+// Device scratch freed on every exit.
+struct Scratch {
+    std::vector<void*> p;
+    ~Scratch() {
+        for (void* q : p) cudaFree(q);
+    }
+    template <typename X>
+    int get(X** x, size_t bytes) {
+        void* q = nullptr;
+        if (cudaMalloc(&q, std::max<size_t>(bytes, 16)) != cudaSuccess) return GBK_OUT_OF_MEMORY;
+        p.push_back(q);
+        *x = (X*)q;
+        return GBK_SUCCESS;
+    }
+};
+
+// Products per block: keys, values and their sorted copies, about 24 bytes
+// each.  GBK_MXM_BLOCK_PRODUCTS (at least 1) overrides it, so small products
+// can exercise several blocks.
+constexpr int64_t kBlockProductsDefault = 64ll << 20;
+
+int64_t block_products() {
+    const char* e = getenv("GBK_MXM_BLOCK_PRODUCTS");
+    const long long v = e ? atoll(e) : 0;
+    return v >= 1 ? (int64_t)v : kBlockProductsDefault;
+}
+
+template <int SR, typename T>
+int mxm_unmasked(gbk_matrix* out, const CsrView& a, const CsrView& b, cudaStream_t s) {
+    const int64_t n = a.nrows, m = b.ncols, annz = a.nnz;
+    Scratch dev;
+    auto need = [&](int rc) { return rc == GBK_SUCCESS; };
+    int64_t* off = nullptr;
+    int32_t* arow = nullptr;
+    if (!need(dev.get(&off, 8 * (annz + 1))) || !need(dev.get(&arow, 4 * annz))) {
+        set_error("gbk_mxm: out of device memory");
+        return GBK_OUT_OF_MEMORY;
+    }
+    if (annz > 0) {
+        k_entry_products<<<nb(annz), 256, 0, s>>>(a.idx, annz, b.ptr, off);
+        GBK_LAUNCHED();
+        k_entry_rows<<<nb(annz), 256, 0, s>>>(a.ptr, n, annz, arow);
+        GBK_LAUNCHED();
+    }
+    GBK_CUDA(cudaMemsetAsync(off + annz, 0, 8, s));
+    {
+        size_t tb = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tb, off, off, annz + 1, s);
+        void* tmp = nullptr;
+        if (!need(dev.get(&tmp, tb))) return GBK_OUT_OF_MEMORY;
+        GBK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, off, off, annz + 1, s));
+        count_launch(1);
+    }
+    // product offsets at row starts, on the host, to cut row blocks
+    int64_t* roff = nullptr;
+    if (!need(dev.get(&roff, 8 * (n + 1)))) return GBK_OUT_OF_MEMORY;
+    k_row_offsets<<<nb(n + 1), 256, 0, s>>>(a.ptr, n, off, roff);
+    GBK_LAUNCHED();
+    std::vector<int32_t> hptr(n + 1);
+    std::vector<int64_t> hroff(n + 1);
+    GBK_CUDA(cudaMemcpyAsync(hptr.data(), a.ptr, 4 * (n + 1), cudaMemcpyDeviceToHost, s));
+    GBK_CUDA(cudaMemcpyAsync(hroff.data(), roff, 8 * (n + 1), cudaMemcpyDeviceToHost, s));
+    GBK_CUDA(cudaStreamSynchronize(s));
+    // blocks of whole rows with at most kBlockProducts products (a single row may exceed it)
+    std::vector<int64_t> cuts{0};
+    const int64_t kBlockProducts = block_products();
+    {
+        int64_t r = 0;
+        while (r < n) {
+            const int64_t base = hroff[r];
+            int64_t r1 = r + 1;
+            int64_t lo = r + 1, hi = n;  // furthest row end within the budget
+            while (lo <= hi) {
+                const int64_t mid = (lo + hi) / 2;
+                if (hroff[mid] - base <= kBlockProducts) {
+                    r1 = mid;
+                    lo = mid + 1;
+                } else {
+                    hi = mid - 1;
+                }
+            }
+            cuts.push_back(r1);
+            r = r1;
+        }
+    }
+    int64_t maxp = 0;
+    for (size_t c = 0; c + 1 < cuts.size(); ++c)
+        maxp = std::max<int64_t>(maxp, hroff[cuts[c + 1]] - hroff[cuts[c]]);
+    unsigned long long *key = nullptr, *key2 = nullptr;
+    T *val = nullptr, *val2 = nullptr;
+    int64_t* nsel = nullptr;
+    if (!need(dev.get(&key, 8 * maxp)) || !need(dev.get(&key2, 8 * maxp)) || !need(dev.get(&val, sizeof(T) * maxp)) ||
+        !need(dev.get(&val2, sizeof(T) * maxp)) || !need(dev.get(&nsel, 16))) {
+        set_error("gbk_mxm: out of device memory for %lld products per block", (long long)maxp);
+        return GBK_OUT_OF_MEMORY;
+    }
+    // scratch sized for the largest block
+    size_t t_sort = 0, t_red = 0, t_sel = 0;
+    int rowbits = 1;
+    while ((1ll << rowbits) < n) ++rowbits;
+    cub::DeviceRadixSort::SortPairs(nullptr, t_sort, key, key2, val, val2, maxp, 0, 32 + rowbits, s);
+    cub::DeviceReduce::ReduceByKey(nullptr, t_red, key2, key, val2, val, nsel, SemiringAdd<SR, T>(), maxp, s);
+    uint8_t* flag = nullptr;
+    if (!need(dev.get(&flag, maxp))) return GBK_OUT_OF_MEMORY;
+    cub::DeviceSelect::Flagged(nullptr, t_sel, key, flag, key2, nsel + 1, maxp, s);
+    size_t t_if = 0;
+    cub::DeviceSelect::If(nullptr, t_if, val, val2, nsel, maxp, NonZero<T>(), s);
+    void* tmp = nullptr;
+    const size_t tbytes = std::max(std::max(t_sort, t_red), std::max(t_sel, t_if)) + 256;
+    if (!need(dev.get(&tmp, tbytes))) return GBK_OUT_OF_MEMORY;
+    // per block: expand, sort, reduce, drop zeros; the kept entries are appended
+    std::vector<unsigned long long*> okeys;
+    std::vector<T*> ovals;
+    std::vector<int64_t> ocnt;
+    struct OutFree {
+        std::vector<unsigned long long*>* k;
+        std::vector<T*>* v;
+        ~OutFree() {
+            for (auto* q : *k) cudaFree(q);
+            for (auto* q : *v) cudaFree(q);
+        }
+    } ofree{&okeys, &ovals};
+    int64_t total = 0;
+    for (size_t c = 0; c + 1 < cuts.size(); ++c) {
+        const int64_t e0 = hptr[cuts[c]], e1 = hptr[cuts[c + 1]];
+        const int64_t p0 = hroff[cuts[c]], p1 = hroff[cuts[c + 1]], np = p1 - p0;
+        if (np == 0) continue;
+        const unsigned grid = (unsigned)std::min<int64_t>(nb(np), (int64_t)num_sms() * 32);
+        k_expand<SR, T><<<grid, 256, 0, s>>>(off, e0, e1, p0, p1, arow, a.idx, (const T*)a.val, b.ptr, b.idx,
+                                             (const T*)b.val, key, val);
+        GBK_LAUNCHED();
+        size_t tb = tbytes;
+        GBK_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, key, key2, val, val2, np, 0, 32 + rowbits, s));
+        tb = tbytes;
+        GBK_CUDA(cub::DeviceReduce::ReduceByKey(tmp, tb, key2, key, val2, val, nsel, SemiringAdd<SR, T>(), np, s));
+        count_launch(2);
+        int64_t nu = 0;
+        GBK_CUDA(cudaMemcpyAsync(&nu, nsel, 8, cudaMemcpyDeviceToHost, s));
+        GBK_CUDA(cudaStreamSynchronize(s));
+        // drop the zero sums (keys and values compacted by the same flags)
+        {
+            unsigned long long* kk = nullptr;
+            T* vv = nullptr;
+            GBK_CUDA(cudaMalloc(&kk, 8 * std::max<int64_t>(nu, 1)));
+            okeys.push_back(kk);
+            GBK_CUDA(cudaMalloc(&vv, sizeof(T) * std::max<int64_t>(nu, 1)));
+            ovals.push_back(vv);
+            tb = tbytes;
+            GBK_CUDA(cub::DeviceSelect::If(tmp, tb, val, vv, nsel, nu, NonZero<T>(), s));
+            count_launch(1);
+            // the same selection for the keys: flags from the values
+            k_nonzero_flags<T><<<nb(nu), 256, 0, s>>>(val, nu, flag);
+            GBK_LAUNCHED();
+            tb = tbytes;
+            GBK_CUDA(cub::DeviceSelect::Flagged(tmp, tb, key, flag, kk, nsel + 1, nu, s));
+            count_launch(1);
+            int64_t kept[2] = {0, 0};
+            GBK_CUDA(cudaMemcpyAsync(kept, nsel, 16, cudaMemcpyDeviceToHost, s));
+            GBK_CUDA(cudaStreamSynchronize(s));
+            ocnt.push_back(kept[0]);
+            total += kept[0];
+        }
+    }
+    GBK_REQUIRE(total < INT32_MAX, GBK_INVALID_VALUE, "gbk_mxm: the product has %lld entries (int32 limit)",
+                (long long)total);
+    // CSR of the result
+    int32_t *row = nullptr, *col = nullptr, *ptr = nullptr;
+    T* cval = nullptr;
+    if (!need(dev.get(&row, 4 * total)) || !need(dev.get(&col, 4 * total)) || !need(dev.get(&ptr, 4 * (n + 1))) ||
+        !need(dev.get(&cval, sizeof(T) * total))) {
+        set_error("gbk_mxm: out of device memory for the result");
+        return GBK_OUT_OF_MEMORY;
+    }
+    int64_t at = 0;
+    for (size_t c = 0; c < okeys.size(); ++c) {
+        if (ocnt[c] > 0) {
+            k_split_keys<<<nb(ocnt[c]), 256, 0, s>>>(okeys[c], ocnt[c], row + at, col + at);
+            GBK_LAUNCHED();
+            GBK_CUDA(cudaMemcpyAsync(cval + at, ovals[c], sizeof(T) * ocnt[c], cudaMemcpyDeviceToDevice, s));
+        }
+        at += ocnt[c];
+    }
+    k_bounds<<<nb(total + 1), 256, 0, s>>>(row, total, n, ptr);
+    GBK_LAUNCHED();
+    GBK_CUDA(cudaStreamSynchronize(s));
+    return gbk_matrix_create_csr(out, n, m, total, ptr, col, cval, std::is_same<T, float>::value ? GBK_F32 : GBK_I32,
+                                 1, s);
+}
+
 }  // namespace
 
 }  // namespace gbk
 
 using namespace gbk;
+
+extern "C" int gbk_mxm(gbk_matrix* out, gbk_matrix A, gbk_matrix B, gbk_semiring sr, void* stream) {
+    GBK_REQUIRE(out && A && B, GBK_NULL_POINTER, "gbk_mxm: NULL argument");
+    GBK_REQUIRE(A->vtype == B->vtype, GBK_DOMAIN_MISMATCH, "gbk_mxm: A and B value types differ");
+    GBK_REQUIRE(A->csr.ncols == B->csr.nrows, GBK_DIMENSION_MISMATCH, "gbk_mxm: A is %lldx%lld, B %lldx%lld",
+                (long long)A->csr.nrows, (long long)A->csr.ncols, (long long)B->csr.nrows, (long long)B->csr.ncols);
+    cudaStream_t s = (cudaStream_t)stream;
+#define MXM_CASE(SRV)                                                                                 \
+    case SRV:                                                                                         \
+        return A->vtype == GBK_F32 ? mxm_unmasked<SRV, float>(out, A->csr, B->csr, s)                 \
+                                   : mxm_unmasked<SRV, int32_t>(out, A->csr, B->csr, s);
+    switch (sr) {
+        MXM_CASE(GBK_PLUS_TIMES)
+        MXM_CASE(GBK_PLUS_SECOND)
+        MXM_CASE(GBK_PLUS_ONE)
+        MXM_CASE(GBK_MIN_PLUS)
+        MXM_CASE(GBK_MIN_SECOND)
+        MXM_CASE(GBK_LOR_LAND)
+        default:
+            set_error("gbk_mxm: semiring %d not provided (plus-times, plus-second, plus-one, min-plus, "
+                      "min-second, or-and)",
+                      (int)sr);
+            return GBK_UNSUPPORTED;
+    }
+#undef MXM_CASE
+}
 
 extern "C" int gbk_mxm_masked(gbk_matrix* out, gbk_matrix M, gbk_matrix A, gbk_matrix B, gbk_semiring sr,
                               gbk_dtype ctype, void* stream) {

@@ -641,3 +641,126 @@ int gbk_reduce(gbk_monoid monoid, gbk_dtype rt, const void* u, gbk_dtype ut, int
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// select (src/backend/operations/select.h)
+
+namespace gbk {
+namespace {
+
+// Does the index-unary operator keep an entry with value x at (i, j)?
+__device__ __forceinline__ bool select_keeps(int op, int64_t i, int64_t j, double x, double k) {
+    const int64_t ki = (int64_t)k;
+    switch (op) {
+        case GBK_SEL_TRIL: return j <= i + ki;
+        case GBK_SEL_TRIU: return j >= i + ki;
+        case GBK_SEL_DIAG: return j == i + ki;
+        case GBK_SEL_OFFDIAG: return j != i + ki;
+        case GBK_SEL_VALUE_EQ: return x == k;
+        case GBK_SEL_VALUE_NE: return x != k;
+        case GBK_SEL_VALUE_GT: return x > k;
+        case GBK_SEL_VALUE_GE: return x >= k;
+        case GBK_SEL_VALUE_LT: return x < k;
+        case GBK_SEL_VALUE_LE: return x <= k;
+    }
+    return false;
+}
+
+template <typename T>
+__global__ void k_select_matrix(const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                const T* __restrict__ val, int64_t nrows, int64_t nnz, int op, double k,
+                                T* __restrict__ out) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    int64_t lo = 0, hi = nrows;  // row of entry e
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (ptr[mid] <= e)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    out[e] = select_keeps(op, lo, idx[e], (double)val[e], k) ? val[e] : T(0);
+}
+
+template <typename OT>
+__global__ void k_select_vector(int op, double k, void* w, int wt, const void* u, int ut, int64_t n, int accum,
+                                const void* mask, int mdt, int comp, int replace) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        bool sel = true;
+        if (mask) sel = (ld_as<double>(mask, mdt, i) != 0.0) != (comp != 0);
+        if (sel) {
+            const OT x = ld_as<OT>(u, ut, i);
+            const OT r = select_keeps(op, i, 0, (double)x, k) ? x : OT(0);
+            st_as<OT>(w, wt, i, binop_any<OT>(accum, ld_as<OT>(w, wt, i), r));
+        } else if (replace) {
+            st_as<OT>(w, wt, i, OT(0));
+        }
+    }
+}
+
+}  // namespace
+}  // namespace gbk
+
+extern "C" int gbk_select_matrix(gbk_matrix* out, gbk_matrix A, gbk_select_op op, double thunk, void* stream) {
+    using namespace gbk;
+    GBK_REQUIRE(out && A, GBK_NULL_POINTER, "gbk_select_matrix: NULL argument");
+    GBK_REQUIRE(op >= GBK_SEL_TRIL && op <= GBK_SEL_VALUE_LE, GBK_INVALID_VALUE, "gbk_select_matrix: bad operator %d",
+                (int)op);
+    cudaStream_t s = (cudaStream_t)stream;
+    const CsrView& v = A->csr;
+    void* vals = nullptr;
+    GBK_CUDA(cudaMalloc(&vals, 4 * (v.nnz > 0 ? v.nnz : 1)));
+    if (v.nnz > 0) {
+        if (A->vtype == GBK_F32)
+            k_select_matrix<float><<<(unsigned)((v.nnz + 255) / 256), 256, 0, s>>>(
+                v.ptr, v.idx, (const float*)v.val, v.nrows, v.nnz, (int)op, thunk, (float*)vals);
+        else
+            k_select_matrix<int32_t><<<(unsigned)((v.nnz + 255) / 256), 256, 0, s>>>(
+                v.ptr, v.idx, (const int32_t*)v.val, v.nrows, v.nnz, (int)op, thunk, (int32_t*)vals);
+        count_launch(1);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            cudaFree(vals);
+            return cuda_fail(e, "select kernel", __FILE__, __LINE__);
+        }
+    }
+    const int rc = gbk_matrix_create_csr(out, v.nrows, v.ncols, v.nnz, v.ptr, v.idx, vals, A->vtype, 1, stream);
+    cudaStreamSynchronize(s);
+    cudaFree(vals);
+    return rc;
+}
+
+extern "C" int gbk_select_vector(gbk_select_op op, double thunk, void* w, gbk_dtype wt, const void* u, gbk_dtype ut,
+                                 int64_t n, gbk_binop accum, const gbk_mask* mask, int replace, void* stream) {
+    using namespace gbk;
+    if (n == 0) return GBK_SUCCESS;
+    GBK_REQUIRE(w && u, GBK_NULL_POINTER, "gbk_select_vector: NULL vector");
+    GBK_REQUIRE(op >= GBK_SEL_TRIL && op <= GBK_SEL_VALUE_LE, GBK_INVALID_VALUE, "gbk_select_vector: bad operator %d",
+                (int)op);
+    cudaStream_t s = (cudaStream_t)stream;
+    MaskArgs m = mask_args(mask);
+    uint8_t* expanded = nullptr;
+    if (m.form == 2) {  // a sparse mask selects its ids (as a structure)
+        int rc = expand_sparse_mask(m, n, &expanded, s);
+        if (rc) return rc;
+        m.dense = expanded;
+        m.dtype = GBK_BOOL;
+        m.form = 1;
+    }
+    const int comp = m.form && (m.mode == GBK_MASK_COMP || m.mode == GBK_MASK_SCMP || m.mode == GBK_MASK_STR_COMP);
+    const unsigned grid = (unsigned)std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 16);
+    const int ot = (is_float(wt) || is_float(ut)) ? GBK_F64 : GBK_I64;
+    if (ot == GBK_F64)
+        k_select_vector<double><<<grid, 256, 0, s>>>((int)op, thunk, w, wt, u, ut, n, (int)accum,
+                                                     m.form ? m.dense : nullptr, m.dtype, comp, replace);
+    else
+        k_select_vector<int64_t><<<grid, 256, 0, s>>>((int)op, thunk, w, wt, u, ut, n, (int)accum,
+                                                      m.form ? m.dense : nullptr, m.dtype, comp, replace);
+    count_launch(1);
+    cudaError_t e = cudaGetLastError();
+    if (expanded) cudaFreeAsync(expanded, s);
+    if (e != cudaSuccess) return cuda_fail(e, "select kernel", __FILE__, __LINE__);
+    return GBK_SUCCESS;
+}

@@ -174,6 +174,17 @@ LA_Info GrB_mxm(lablas::Matrix<W>* c, const lablas::Matrix<M>* mask, A accum, S 
                 const lablas::Matrix<a>* b, lablas::Descriptor* desc) {
     return lablas::mxm(c, mask, accum, op, a_, b, desc);
 }
+// GrB_select (src/cblas_wrappers/operations.hpp:189-230): tagged operators only (lablas::TrilSelect, ...)
+template <typename W, typename M, typename U, typename T, typename A, typename S>
+LA_Info GrB_select(lablas::Vector<W>* w, const lablas::Vector<M>* mask, A accum, S op, const lablas::Vector<U>* u,
+                   const T val, lablas::Descriptor* desc) {
+    return lablas::select(w, mask, accum, op, u, val, desc);
+}
+template <typename W, typename M, typename U, typename T, typename A, typename S>
+LA_Info GrB_select(lablas::Matrix<W>* w, const lablas::Matrix<M>* mask, A accum, S op, const lablas::Matrix<U>* u,
+                   const T val, lablas::Descriptor* desc) {
+    return lablas::select(w, mask, accum, op, u, val, desc);
+}
 template <typename T, typename U, typename A, typename Mon>
 LA_Info GrB_reduce(T* val, A accum, Mon op, const lablas::Vector<U>* u, lablas::Descriptor* desc) {
     return lablas::reduce(val, accum, op, u, desc);

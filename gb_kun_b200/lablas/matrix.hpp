@@ -123,8 +123,17 @@ public:
     // every value is 1.  Throws on a missing or malformed file.
     void init_from_mtx(const std::string& name) {
         release();
-        int rc = gbk_matrix_create_from_file(&h_, name.c_str(), dtype, stream());
+        gbk_matrix h = nullptr;
+        int rc = gbk_matrix_create_from_file(&h, name.c_str(), dtype, stream());
         throw_if(rc, "init_from_mtx");
+        adopt_handle(h);
+    }
+
+    // Take over a device matrix made by the library (SpGEMM, select, a file)
+    // and download its host copy; rows keep the device's order.
+    LA_Info adopt_handle(gbk_matrix h) {
+        release();
+        h_ = h;
         gbk_matrix_info inf;
         gbk_matrix_get_info(h_, &inf);
         nrows_ = (Index)inf.nrows;
@@ -133,11 +142,11 @@ public:
         rp_.resize(nrows_ + 1);
         col_.resize(nnz_);
         val_.resize(nnz_);
-        rc = gbk_matrix_download_csr(h_, rp_.data(), col_.data(), val_.data(), stream());
-        throw_if(rc, "init_from_mtx");
+        int rc = gbk_matrix_download_csr(h_, rp_.data(), col_.data(), val_.data(), stream());
+        throw_if(rc, "adopt a device matrix");
         rowdeg_.clear();
         coldeg_.clear();
-        apply_format();
+        return apply_format();
     }
 
     Index* get_rowdegrees() {
@@ -263,6 +272,9 @@ private:
         gbk_format f = GBK_FMT_CSR;
         switch (format_) {
             case CSR: f = GBK_FMT_CSR; break;
+            // COO (spmv_coo.h) holds the same entries in row order: stored as CSR, the
+            // SpMV gives its results without its unsynchronised updates of shared rows
+            case COO: f = GBK_FMT_CSR; break;
             case CSR_SEG: f = GBK_FMT_CSR_SEG; break;
             case LAV: f = GBK_FMT_LAV; break;
             case SELL_C: f = GBK_FMT_SELL_C; break;

@@ -380,8 +380,13 @@ LA_Info mxm(Matrix<c>* C, const Matrix<m>* mask, BinaryOpT accum, SemiringT op, 
     if (detail::null_any(C, A, B, desc)) return GrB_UNINITIALIZED_OBJECT;
     Desc_value mm = mask_mode(desc);
     if (mm == GrB_COMP || mm == GrB_STR_COMP) throw "Error: complementary mask is not supported yet";
-    if (!mask) return GrB_INVALID_VALUE;  // unmasked SpGEMM is not provided on the device
     gbk_matrix out = nullptr;
+    if (!mask) {  // unmasked: SpMSpM_unmasked_ikj (spmspm_hash_based_gustavson.h:9-148)
+        if (!std::is_same<c, a>::value || !std::is_same<a, b>::value) return GrB_DOMAIN_MISMATCH;
+        int rc = gbk_mxm(&out, A->handle(), B->handle(), SemiringT::gbk_sr, stream());
+        if (rc) return detail::done(rc);
+        return C->adopt_handle(out);
+    }
     int rc = gbk_mxm_masked(&out, mask->handle(), A->handle(), B->handle(), SemiringT::gbk_sr,
                             dtype_of<c>::value, stream());
     if (rc) return detail::done(rc);
@@ -392,6 +397,65 @@ template <typename c, typename m, typename a, typename b, typename SemiringT>
 LA_Info mxm(Matrix<c>* C, const Matrix<m>* mask, NULL_TYPE, SemiringT op, const Matrix<a>* A, const Matrix<b>* B,
             Descriptor* desc) {
     return mxm(C, mask, second<c, a, b>(), op, A, B, desc);
+}
+
+// ---------------------------------------------------------------------------
+// select (select.h): tagged index-unary operators only (lablas::TrilSelect,
+// TriuSelect, DiagSelect, OffdiagSelect, Value*Select); a generic callable
+// cannot run on the device.
+
+/* Matrix: same structure as u, values op(u_ij, i, j, val) (select.h:363-395,
+ * which accumulates into 0, so the accumulator and the mask do not act). */
+template <typename W, typename M, typename U, typename T, typename BinaryOpT, typename SelectOpT>
+LA_Info select(Matrix<W>* w, const Matrix<M>* mask, BinaryOpT accum, SelectOpT op, const Matrix<U>* u, const T val,
+               Descriptor* desc) {
+    static_assert(is_select_op<SelectOpT>::value,
+                  "select on the device takes a tagged operator: lablas::TrilSelect, TriuSelect, DiagSelect, "
+                  "OffdiagSelect, ValueEq/Ne/Gt/Ge/Lt/LeSelect");
+    static_assert(std::is_same<W, U>::value, "select keeps the value type of u");
+    (void)mask;
+    (void)accum;
+    (void)op;
+    (void)desc;
+    if (detail::null_any(w, u)) return GrB_UNINITIALIZED_OBJECT;
+    gbk_matrix out = nullptr;
+    int rc = gbk_select_matrix(&out, u->handle(), SelectOpT::gbk_sel, (double)val, stream());
+    if (rc) return detail::done(rc);
+    return w->adopt_handle(out);
+}
+template <typename W, typename M, typename U, typename T, typename SelectOpT>
+LA_Info select(Matrix<W>* w, const Matrix<M>* mask, NULL_TYPE, SelectOpT op, const Matrix<U>* u, const T val,
+               Descriptor* desc) {
+    return select(w, mask, second<W, U, W>(), op, u, val, desc);
+}
+
+/* Vector: w[i] = accum(w[i], op(u[i], i, 0, val)) where the mask selects;
+ * GrB_REPLACE zeroes the rest (select.h:17-315). */
+template <typename W, typename M, typename U, typename T, typename BinaryOpT, typename SelectOpT>
+LA_Info select(Vector<W>* w, const Vector<M>* mask, BinaryOpT accum, SelectOpT op, const Vector<U>* u, const T val,
+               Descriptor* desc) {
+    static_assert(is_select_op<SelectOpT>::value,
+                  "select on the device takes a tagged operator: lablas::TrilSelect, TriuSelect, DiagSelect, "
+                  "OffdiagSelect, ValueEq/Ne/Gt/Ge/Lt/LeSelect");
+    (void)accum;
+    (void)op;
+    if (detail::null_any(w, u)) return GrB_UNINITIALIZED_OBJECT;
+    if (w->size() != u->size()) return GrB_DIMENSION_MISMATCH;
+    if (mask && mask->size() != w->size()) return GrB_DIMENSION_MISMATCH;
+    const U* up = u->dense_ptr();
+    W* wp = w->dense_ptr();
+    gbk_mask m{};
+    if (mask) m = detail::mask_arg(mask, desc);
+    Desc_value out_mode = GrB_DEFAULT;
+    if (desc) desc->get(GrB_OUTPUT, &out_mode);
+    return detail::done(gbk_select_vector(SelectOpT::gbk_sel, (double)val, wp, Vector<W>::dtype, up,
+                                          Vector<U>::dtype, w->size(), BinaryOpT::gbk_code, mask ? &m : nullptr,
+                                          mask && out_mode == GrB_REPLACE, stream()));
+}
+template <typename W, typename M, typename U, typename T, typename SelectOpT>
+LA_Info select(Vector<W>* w, const Vector<M>* mask, NULL_TYPE, SelectOpT op, const Vector<U>* u, const T val,
+               Descriptor* desc) {
+    return select(w, mask, second<W, U, W>(), op, u, val, desc);
 }
 
 // ---------------------------------------------------------------------------

@@ -222,6 +222,35 @@ GBK_SEMIRING(PlusOneSemiring, PlusMonoid, GrB_ONEB_T, GBK_PLUS_ONE)
 template <typename T, typename = void> struct is_semiring : std::false_type {};
 template <typename T> struct is_semiring<T, std::void_t<decltype(T::gbk_sr)>> : std::true_type {};
 
+// Index-unary select operators (the GraphBLAS GrB_TRIL ... GrB_VALUELE
+// family), tagged with their C-ABI code: op(x, i, j, k) returns x where the
+// operator keeps the entry and 0 where not, the convention of the
+// reference's select lambdas (algorithms/tc/tc.hpp:55-70).
+#define GBK_SELECT_OP(NAME, CODE, KEEP)                                                         \
+    template <typename T>                                                                      \
+    struct NAME {                                                                              \
+        static constexpr gbk_select_op gbk_sel = CODE;                                         \
+        inline T operator()(T x, long long i, long long j, double k) const {                   \
+            (void)i;                                                                           \
+            (void)j;                                                                           \
+            return (KEEP) ? x : T(0);                                                          \
+        }                                                                                      \
+    };
+GBK_SELECT_OP(TrilSelect, GBK_SEL_TRIL, (double)j <= (double)i + k)
+GBK_SELECT_OP(TriuSelect, GBK_SEL_TRIU, (double)j >= (double)i + k)
+GBK_SELECT_OP(DiagSelect, GBK_SEL_DIAG, (double)j == (double)i + k)
+GBK_SELECT_OP(OffdiagSelect, GBK_SEL_OFFDIAG, (double)j != (double)i + k)
+GBK_SELECT_OP(ValueEqSelect, GBK_SEL_VALUE_EQ, (double)x == k)
+GBK_SELECT_OP(ValueNeSelect, GBK_SEL_VALUE_NE, (double)x != k)
+GBK_SELECT_OP(ValueGtSelect, GBK_SEL_VALUE_GT, (double)x > k)
+GBK_SELECT_OP(ValueGeSelect, GBK_SEL_VALUE_GE, (double)x >= k)
+GBK_SELECT_OP(ValueLtSelect, GBK_SEL_VALUE_LT, (double)x < k)
+GBK_SELECT_OP(ValueLeSelect, GBK_SEL_VALUE_LE, (double)x <= k)
+#undef GBK_SELECT_OP
+
+template <typename T, typename = void> struct is_select_op : std::false_type {};
+template <typename T> struct is_select_op<T, std::void_t<decltype(T::gbk_sel)>> : std::true_type {};
+
 template <typename Op> constexpr gbk_binop ewise_add_code() {
     if constexpr (is_semiring<Op>::value) return Op::gbk_add;
     else return Op::gbk_code;

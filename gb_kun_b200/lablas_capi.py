@@ -39,6 +39,7 @@ def lib():
         L.gbk_lablas_pagerank.argtypes = [vp, i32, C.c_double, C.c_double, vp, C.POINTER(i32), dp]
         L.gbk_lablas_ppr.argtypes = [vp, i64, i32, C.c_double, C.c_double, vp, C.POINTER(i32), dp]
         L.gbk_lablas_tc.argtypes = [vp, C.POINTER(C.c_uint64), dp]
+        L.gbk_lablas_tc_method.argtypes = [vp, i32, C.POINTER(C.c_uint64), dp]
         L.gbk_lablas_spmv.argtypes = [vp, i32, vp, vp, vp, dp]
         _LIB = L
     return _LIB
@@ -137,6 +138,14 @@ class Graph:
         cnt = C.c_uint64()
         ms = C.c_double()
         _check(lib().gbk_lablas_tc(self.h, C.byref(cnt), C.byref(ms)), "tc")
+        return int(cnt.value), ms.value
+
+    def tc_method(self, method):
+        """LAGr_TriangleCount with a method: 0 default, 1 Burkhardt, 2 Cohen, 3 Sandia, 4 Sandia2,
+        5 SandiaDot, 6 SandiaDot2."""
+        cnt = C.c_uint64()
+        ms = C.c_double()
+        _check(lib().gbk_lablas_tc_method(self.h, int(method), C.byref(cnt), C.byref(ms)), "tc_method")
         return int(cnt.value), ms.value
 
     def spmv(self, vals, x, fmt=0):

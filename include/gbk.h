@@ -163,6 +163,45 @@ int gbk_spmspv(gbk_matrix A, int transpose, gbk_semiring sr, gbk_binop accum, gb
 int gbk_mxm_masked(gbk_matrix* out, gbk_matrix M, gbk_matrix A, gbk_matrix B, gbk_semiring sr, gbk_dtype ctype,
                    void* stream);
 
+/* Unmasked SpGEMM C = A (+.x) B, replacing SpMSpM_unmasked_ikj
+ * (src/backend/spmspm/spmspm_hash_based_gustavson.h:9-148, reached by mxm
+ * with a NULL mask, src/backend/operations/operations.h:476-482): every
+ * product A_ik * B_kj is added into C_ij with the semiring's add and entries
+ * whose sum is 0 are dropped (the reference keeps val != 0).  A and B share
+ * a value type (GBK_F32 / GBK_I32), which C takes; rows of C are
+ * column-sorted (the reference's order follows its hash maps).  Semirings:
+ * plus-times, plus-second, plus-one, min-plus, min-second, or-and. */
+int gbk_mxm(gbk_matrix* out, gbk_matrix A, gbk_matrix B, gbk_semiring sr, void* stream);
+
+/* ---- select ---------------------------------------------------------------- */
+
+/* Index-unary operators of select: index ops keep a_ij by position (k = the
+ * thunk), value ops by comparing a_ij with the thunk. */
+typedef enum gbk_select_op {
+    GBK_SEL_TRIL = 0,      /* j <= i + k */
+    GBK_SEL_TRIU = 1,      /* j >= i + k */
+    GBK_SEL_DIAG = 2,      /* j == i + k */
+    GBK_SEL_OFFDIAG = 3,   /* j != i + k */
+    GBK_SEL_VALUE_EQ = 4,
+    GBK_SEL_VALUE_NE = 5,
+    GBK_SEL_VALUE_GT = 6,
+    GBK_SEL_VALUE_GE = 7,
+    GBK_SEL_VALUE_LT = 8,
+    GBK_SEL_VALUE_LE = 9
+} gbk_select_op;
+
+/* Matrix select as backend::select (src/backend/operations/select.h:363-395):
+ * the result keeps every stored entry of A (the structure does not change);
+ * an entry's value is a_ij where the operator keeps it and 0 where not. */
+int gbk_select_matrix(gbk_matrix* out, gbk_matrix A, gbk_select_op op, double thunk, void* stream);
+/* Vector select (select.h:17-315): for every i the mask selects (all i with
+ * mask == NULL; a dense mask selects non-zero entries, a sparse one its ids,
+ * COMP / SCMP / STR_COMP complement), w[i] = accum(w[i], r) with r = u[i]
+ * if the operator keeps (u[i], i, 0) and 0 if not; unselected i get 0 when
+ * replace != 0 (GrB_REPLACE) and keep w[i] otherwise. */
+int gbk_select_vector(gbk_select_op op, double thunk, void* w, gbk_dtype wt, const void* u, gbk_dtype ut,
+                      int64_t n, gbk_binop accum, const gbk_mask* mask, int replace, void* stream);
+
 /* ---- batched traversals (many sources per launch) ----------------------- */
 
 /* Multi-source BFS: up to 64 sources advanced together, one bit of a uint64

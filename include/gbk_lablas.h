@@ -52,6 +52,11 @@ int gbk_lablas_ppr(gbk_lablas_graph g, int64_t seed, int32_t itermax, double dam
                    int32_t* iterations, double* ms);
 /* Burkhardt triangle count (algorithms/tc/tc.hpp:209-217); the graph must be symmetric. */
 int gbk_lablas_tc(gbk_lablas_graph g, uint64_t* count, double* ms);
+/* LAGr_TriangleCount with a method (algorithms/tc/tc.hpp:17-26): 0 default,
+ * 1 Burkhardt, 2 Cohen, 3 Sandia, 4 Sandia2, 5 SandiaDot, 6 SandiaDot2;
+ * presort NoSort.  The reference's L / U keep A's structure, so every method
+ * returns its Burkhardt count. */
+int gbk_lablas_tc_method(gbk_lablas_graph g, int32_t method, uint64_t* count, double* ms);
 /* y = A x through lablas::mxv (plus-times, f32) in the given storage format
  * (MatrixStorageFormat value: 0 CSR, 3 CSR_SEG, 4 LAV, 6 SELL_C); vals are
  * the nnz matrix values. */

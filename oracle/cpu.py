@@ -153,6 +153,9 @@ class Reference:
             L.ref_graph_read.argtypes = [C.c_char_p, C.POINTER(i64), C.POINTER(i64), C.POINTER(vp), dp]
             L.ref_graph_csr.argtypes = [vp, vp, vp, vp]
             L.ref_graph_free.argtypes = [vp]
+            L.ref_mxm.argtypes = [C.c_int, i64, vp, vp, vp, C.POINTER(vp), C.POINTER(i64), dp]
+            L.ref_tc_method.argtypes = [C.c_int, i64, vp, vp, vp, dp]
+            L.ref_select_matrix.argtypes = [C.c_int, C.c_double, i64, vp, vp, vp, C.POINTER(vp)]
 
     @staticmethod
     def available() -> bool:
@@ -224,3 +227,37 @@ class Reference:
         finally:
             self.L.ref_graph_free(h)
         return n.value, rp, col[:z.value], val[:z.value], ms.value
+
+    def _take_matrix(self, h, n, nnz):
+        """(row_ptr, col, val) of a reference matrix (n rows, nnz entries) behind handle h, freed afterwards."""
+        try:
+            rp = np.empty(n + 1, np.int32)
+            col = np.empty(max(nnz, 1), np.int32)
+            val = np.empty(max(nnz, 1), np.float32)
+            self.L.ref_graph_csr(h, _p(rp), _p(col), _p(val))
+        finally:
+            self.L.ref_graph_free(h)
+        return rp, col[:nnz], val[:nnz]
+
+    def mxm(self, g, val, semiring=0):
+        """The reference's unmasked A (+.x) A: (row_ptr, col, val, ms), rows in its hash-map order."""
+        h, z, ms = C.c_void_p(), C.c_int64(0), C.c_double(0)
+        rc = self.L.ref_mxm(semiring, g.n, _p(g.row_ptr), _p(g.col), _p(val), C.byref(h), C.byref(z), C.byref(ms))
+        if rc:
+            raise RuntimeError(f"ref_mxm rc={rc}")
+        rp, col, v = self._take_matrix(h, g.n, z.value)
+        return rp, col, v, ms.value
+
+    def select_matrix(self, g, val, op, thunk):
+        h = C.c_void_p()
+        rc = self.L.ref_select_matrix(op, float(thunk), g.n, _p(g.row_ptr), _p(g.col), _p(val), C.byref(h))
+        if rc:
+            raise RuntimeError(f"ref_select_matrix rc={rc}")
+        return self._take_matrix(h, g.n, g.nnz)
+
+    def tc_method(self, g, method):
+        cnt, ms = C.c_uint64(0), C.c_double(0)
+        rc = self.L.ref_tc_method(method, g.n, _p(g.row_ptr), _p(g.col), C.byref(cnt), C.byref(ms))
+        if rc:
+            raise RuntimeError(f"ref_tc_method rc={rc}")
+        return int(cnt.value), ms.value

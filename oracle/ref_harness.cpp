@@ -279,4 +279,109 @@ int ref_graph_csr(void* handle, int32_t* rp, int32_t* col, float* val) {
 
 void ref_graph_free(void* handle) { delete (lablas::Matrix<float>*)handle; }
 
+// Unmasked SpGEMM C = A (+.x) A through the reference's mxm with a NULL
+// mask (src/backend/operations/operations.h:476-482 -> SpMSpM_unmasked_ikj,
+// spmspm_hash_based_gustavson.h:9-148).  semiring (gbk_semiring values):
+// 0 plus-times, 1 or-and, 6 min-plus, 10 plus-one.  C stays alive behind
+// *handle (read it with ref_graph_csr, free it with ref_graph_free).
+int ref_mxm(int semiring, int64_t n, const int32_t* rp, const int32_t* col, const float* val, void** handle,
+            int64_t* nnz, double* ms) {
+    try {
+        Quiet q;
+        lablas::Matrix<float> A;
+        build(A, 0, n, rp, col, val);
+        auto* C = new lablas::Matrix<float>();
+        lablas::Descriptor desc;
+        const lablas::Matrix<float>* nomask = nullptr;
+        const auto acc = lablas::second<float, float, float>();
+        LA_Info rc = GrB_SUCCESS;
+        const double t0 = now_ms();
+        switch (semiring) {
+            case 0: rc = lablas::mxm(C, nomask, acc, lablas::PlusMultipliesSemiring<float>(), &A, &A, &desc); break;
+            case 1: rc = lablas::mxm(C, nomask, acc, lablas::LogicalOrAndSemiring<float>(), &A, &A, &desc); break;
+            case 6: rc = lablas::mxm(C, nomask, acc, lablas::MinimumPlusSemiring<float>(), &A, &A, &desc); break;
+            case 10: rc = lablas::mxm(C, nomask, acc, lablas::PlusOneSemiring<float>(), &A, &A, &desc); break;
+            default: delete C; return 5;
+        }
+        if (ms) *ms = now_ms() - t0;
+        if (rc != GrB_SUCCESS) {
+            delete C;
+            return (int)rc;
+        }
+        *nnz = (int64_t)C->get_matrix()->get_csr()->get_nnz();
+        *handle = C;
+        return 0;
+    } catch (const char* e) {
+        std::cerr << "reference error: " << e << std::endl;
+        return 13;
+    }
+}
+
+// Matrix select through the reference's select (select.h:363-395) with an
+// index-unary operator (gbk_select_op values): 0 tril, 1 triu, 2 diag,
+// 3 offdiag (k = thunk), 4..9 value ==, !=, >, >=, <, <= thunk; the
+// operator returns the value where it keeps the entry and 0 elsewhere.
+int ref_select_matrix(int op, double thunk, int64_t n, const int32_t* rp, const int32_t* col, const float* val,
+                      void** handle) {
+    try {
+        Quiet q;
+        lablas::Matrix<float> U;
+        build(U, 0, n, rp, col, val);
+        auto* W = new lablas::Matrix<float>();
+        const lablas::Matrix<float>* nomask = nullptr;
+        lablas::Descriptor desc;
+        const auto acc = lablas::second<float, float, float>();
+        auto sel = [op](float x, Index i, Index j, double k) -> float {
+            const Index ki = (Index)k;
+            bool keep = false;
+            switch (op) {
+                case 0: keep = j <= i + ki; break;
+                case 1: keep = j >= i + ki; break;
+                case 2: keep = j == i + ki; break;
+                case 3: keep = j != i + ki; break;
+                case 4: keep = x == k; break;
+                case 5: keep = x != k; break;
+                case 6: keep = x > k; break;
+                case 7: keep = x >= k; break;
+                case 8: keep = x < k; break;
+                case 9: keep = x <= k; break;
+            }
+            return keep ? x : 0.0f;
+        };
+        LA_Info rc = lablas::select(W, nomask, acc, sel, &U, thunk, &desc);
+        if (rc != GrB_SUCCESS) {
+            delete W;
+            return (int)rc;
+        }
+        *handle = W;
+        return 0;
+    } catch (const char* e) {
+        std::cerr << "reference error: " << e << std::endl;
+        return 13;
+    }
+}
+
+// LAGr_TriangleCount with a method (algorithms/tc/tc.hpp:17-26), NoSort,
+// masked IKJ SpGEMM as the default descriptor.
+int ref_tc_method(int method, int64_t n, const int32_t* rp, const int32_t* col, uint64_t* count, double* ms) {
+    try {
+        Quiet q;
+        std::vector<int> ones(rp[n], 1);
+        lablas::Matrix<int> A;
+        build(A, 0, n, rp, col, ones.data());
+        LAGraph_Graph<int> graph(A);
+        uint64_t ntri = 0;
+        const double t0 = now_ms();
+        lablas::algorithm::LAGr_TriangleCount(&ntri, &graph, (lablas::algorithm::LAGraph_TriangleCount_Method)method,
+                                              lablas::algorithm::LAGraph_TriangleCount_NoSort,
+                                              &lablas::GrB_DESC_IKJ_MASKED);
+        if (ms) *ms = now_ms() - t0;
+        *count = ntri;
+        return 0;
+    } catch (const char* e) {
+        std::cerr << "reference error: " << e << std::endl;
+        return 13;
+    }
+}
+
 }  // extern "C"
