@@ -125,10 +125,12 @@ __global__ void k_entry_rows(const int32_t* __restrict__ aptr, int64_t nrows, in
 }
 
 // Products [p0, p1) of the entries [e0, e1) (off: exclusive product offsets
-// per entry, off[e1] = p1): key (row << 32 | column), value mul(a, b).
+// per entry, off[e1] = p1): key ((row - row0) << colbits | column), value
+// mul(a, b); the short keys keep the radix sort to the bits in use.
 template <int SR, typename T>
 __global__ void k_expand(const int64_t* __restrict__ off, int64_t e0, int64_t e1, int64_t p0, int64_t p1,
-                         const int32_t* __restrict__ arow, const int32_t* __restrict__ aidx, const T* __restrict__ aval,
+                         const int32_t* __restrict__ arow, int32_t row0, int colbits, const int32_t* __restrict__ aidx,
+                         const T* __restrict__ aval,
                          const int32_t* __restrict__ bptr, const int32_t* __restrict__ bidx,
                          const T* __restrict__ bval, unsigned long long* __restrict__ key, T* __restrict__ val) {
     using S = Semiring<SR, T>;
@@ -144,7 +146,7 @@ __global__ void k_expand(const int64_t* __restrict__ off, int64_t e0, int64_t e1
         }
         const int32_t k = aidx[lo];
         const int64_t f = bptr[k] + (p - off[lo]);
-        key[p - p0] = ((unsigned long long)(uint32_t)arow[lo] << 32) | (unsigned long long)(uint32_t)bidx[f];
+        key[p - p0] = ((unsigned long long)(uint32_t)(arow[lo] - row0) << colbits) | (unsigned long long)(uint32_t)bidx[f];
         val[p - p0] = S::mul(aval[lo], bval[f]);
     }
 }
@@ -159,12 +161,12 @@ struct NonZero {
     __device__ __forceinline__ bool operator()(const T& v) const { return v != T(0); }
 };
 
-__global__ void k_split_keys(const unsigned long long* __restrict__ key, int64_t n, int32_t* __restrict__ row,
-                             int32_t* __restrict__ col) {
+__global__ void k_split_keys(const unsigned long long* __restrict__ key, int64_t n, int32_t row0, int colbits,
+                             int32_t* __restrict__ row, int32_t* __restrict__ col) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    row[i] = (int32_t)(key[i] >> 32);
-    col[i] = (int32_t)(key[i] & 0xffffffffu);
+    row[i] = row0 + (int32_t)(key[i] >> colbits);
+    col[i] = (int32_t)(key[i] & ((1ull << colbits) - 1));
 }
 
 // ptr[r] = first entry of row >= r (rows ascending)
@@ -184,16 +186,19 @@ __global__ void k_nonzero_flags(const T* __restrict__ v, int64_t n, uint8_t* __r
 
 unsigned nb(int64_t n) { return (unsigned)std::max<int64_t>(1, (n + 255) / 256); }
 
-// Device scratch freed on every exit.
+// Device scratch from the stream-ordered pool (reused across calls), freed
+// on the stream on every exit.
 struct Scratch {
+    cudaStream_t s;
     std::vector<void*> p;
+    explicit Scratch(cudaStream_t st) : s(st) {}
     ~Scratch() {
-        for (void* q : p) cudaFree(q);
+        for (void* q : p) cudaFreeAsync(q, s);
     }
     template <typename X>
     int get(X** x, size_t bytes) {
         void* q = nullptr;
-        if (cudaMalloc(&q, std::max<size_t>(bytes, 16)) != cudaSuccess) return GBK_OUT_OF_MEMORY;
+        if (cudaMallocAsync(&q, std::max<size_t>(bytes, 16), s) != cudaSuccess) return GBK_OUT_OF_MEMORY;
         p.push_back(q);
         *x = (X*)q;
         return GBK_SUCCESS;
@@ -214,7 +219,7 @@ int64_t block_products() {
 template <int SR, typename T>
 int mxm_unmasked(gbk_matrix* out, const CsrView& a, const CsrView& b, cudaStream_t s) {
     const int64_t n = a.nrows, m = b.ncols, annz = a.nnz;
-    Scratch dev;
+    Scratch dev(s);
     auto need = [&](int rc) { return rc == GBK_SUCCESS; };
     int64_t* off = nullptr;
     int32_t* arow = nullptr;
@@ -284,7 +289,9 @@ int mxm_unmasked(gbk_matrix* out, const CsrView& a, const CsrView& b, cudaStream
     size_t t_sort = 0, t_red = 0, t_sel = 0;
     int rowbits = 1;
     while ((1ll << rowbits) < n) ++rowbits;
-    cub::DeviceRadixSort::SortPairs(nullptr, t_sort, key, key2, val, val2, maxp, 0, 32 + rowbits, s);
+    int colbits = 1;
+    while ((1ll << colbits) < m) ++colbits;
+    cub::DeviceRadixSort::SortPairs(nullptr, t_sort, key, key2, val, val2, maxp, 0, rowbits + colbits, s);
     cub::DeviceReduce::ReduceByKey(nullptr, t_red, key2, key, val2, val, nsel, SemiringAdd<SR, T>(), maxp, s);
     uint8_t* flag = nullptr;
     if (!need(dev.get(&flag, maxp))) return GBK_OUT_OF_MEMORY;
@@ -298,25 +305,20 @@ int mxm_unmasked(gbk_matrix* out, const CsrView& a, const CsrView& b, cudaStream
     std::vector<unsigned long long*> okeys;
     std::vector<T*> ovals;
     std::vector<int64_t> ocnt;
-    struct OutFree {
-        std::vector<unsigned long long*>* k;
-        std::vector<T*>* v;
-        ~OutFree() {
-            for (auto* q : *k) cudaFree(q);
-            for (auto* q : *v) cudaFree(q);
-        }
-    } ofree{&okeys, &ovals};
+    std::vector<int64_t> orow0;  // first row of each kept block
     int64_t total = 0;
     for (size_t c = 0; c + 1 < cuts.size(); ++c) {
         const int64_t e0 = hptr[cuts[c]], e1 = hptr[cuts[c + 1]];
         const int64_t p0 = hroff[cuts[c]], p1 = hroff[cuts[c + 1]], np = p1 - p0;
         if (np == 0) continue;
         const unsigned grid = (unsigned)std::min<int64_t>(nb(np), (int64_t)num_sms() * 32);
-        k_expand<SR, T><<<grid, 256, 0, s>>>(off, e0, e1, p0, p1, arow, a.idx, (const T*)a.val, b.ptr, b.idx,
-                                             (const T*)b.val, key, val);
+        k_expand<SR, T><<<grid, 256, 0, s>>>(off, e0, e1, p0, p1, arow, (int32_t)cuts[c], colbits, a.idx,
+                                             (const T*)a.val, b.ptr, b.idx, (const T*)b.val, key, val);
         GBK_LAUNCHED();
+        int brows = 1;  // bits of the block's row span
+        while ((1ll << brows) < cuts[c + 1] - cuts[c]) ++brows;
         size_t tb = tbytes;
-        GBK_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, key, key2, val, val2, np, 0, 32 + rowbits, s));
+        GBK_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, key, key2, val, val2, np, 0, brows + colbits, s));
         tb = tbytes;
         GBK_CUDA(cub::DeviceReduce::ReduceByKey(tmp, tb, key2, key, val2, val, nsel, SemiringAdd<SR, T>(), np, s));
         count_launch(2);
@@ -327,10 +329,13 @@ int mxm_unmasked(gbk_matrix* out, const CsrView& a, const CsrView& b, cudaStream
         {
             unsigned long long* kk = nullptr;
             T* vv = nullptr;
-            GBK_CUDA(cudaMalloc(&kk, 8 * std::max<int64_t>(nu, 1)));
+            if (!need(dev.get(&kk, 8 * std::max<int64_t>(nu, 1))) || !need(dev.get(&vv, sizeof(T) * std::max<int64_t>(nu, 1)))) {
+                set_error("gbk_mxm: out of device memory for a block's result");
+                return GBK_OUT_OF_MEMORY;
+            }
             okeys.push_back(kk);
-            GBK_CUDA(cudaMalloc(&vv, sizeof(T) * std::max<int64_t>(nu, 1)));
             ovals.push_back(vv);
+            orow0.push_back(cuts[c]);
             tb = tbytes;
             GBK_CUDA(cub::DeviceSelect::If(tmp, tb, val, vv, nsel, nu, NonZero<T>(), s));
             count_launch(1);
@@ -360,7 +365,7 @@ int mxm_unmasked(gbk_matrix* out, const CsrView& a, const CsrView& b, cudaStream
     int64_t at = 0;
     for (size_t c = 0; c < okeys.size(); ++c) {
         if (ocnt[c] > 0) {
-            k_split_keys<<<nb(ocnt[c]), 256, 0, s>>>(okeys[c], ocnt[c], row + at, col + at);
+            k_split_keys<<<nb(ocnt[c]), 256, 0, s>>>(okeys[c], ocnt[c], (int32_t)orow0[c], colbits, row + at, col + at);
             GBK_LAUNCHED();
             GBK_CUDA(cudaMemcpyAsync(cval + at, ovals[c], sizeof(T) * ocnt[c], cudaMemcpyDeviceToDevice, s));
         }
@@ -420,8 +425,8 @@ extern "C" int gbk_mxm_masked(gbk_matrix* out, gbk_matrix M, gbk_matrix A, gbk_m
     const CsrView& m = M->csr;
     const CsrView& a = A->csr;
     const CsrView& b = B->csc;
-    void* vals = nullptr;
-    GBK_CUDA(cudaMalloc(&vals, 4 * (m.nnz > 0 ? m.nnz : 1)));
+    void* vals = nullptr;  // from the stream-ordered pool: results of this size recur (triangle counting)
+    GBK_CUDA(cudaMallocAsync(&vals, 4 * (m.nnz > 0 ? m.nnz : 1), s));
     if (m.nnz > 0) {
         const int threads = 256;
         int64_t groups = (m.nnz + 31) / 32;
@@ -454,6 +459,6 @@ extern "C" int gbk_mxm_masked(gbk_matrix* out, gbk_matrix M, gbk_matrix A, gbk_m
     }
     GBK_CUDA(cudaStreamSynchronize(s));
     rc = gbk_matrix_create_csr(out, m.nrows, m.ncols, m.nnz, m.ptr, m.idx, vals, ctype, 1, stream);
-    cudaFree(vals);
+    cudaFreeAsync(vals, s);
     return rc;
 }
