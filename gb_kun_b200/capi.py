@@ -133,6 +133,7 @@ def _declare(lib):
         "gbk_sssp_multi": ([vp, vp, ci, vp, vp, vp], ci),
         "gbk_batch_autotune": ([vp, ci, vp, ci, C.POINTER(BatchTuneResult), vp], ci),
         "gbk_mxm": ([C.POINTER(vp), vp, vp, ci, vp], ci),
+        "gbk_triangle_count": ([vp, C.POINTER(C.c_uint64), vp], ci),
         "gbk_select_matrix": ([C.POINTER(vp), vp, ci, C.c_double, vp], ci),
         "gbk_select_vector": ([ci, C.c_double, vp, ci, vp, ci, i64, ci, mp, ci, vp], ci),
         "gbk_file_info_read": ([C.c_char_p, C.POINTER(FileInfo)], ci),
@@ -275,6 +276,12 @@ class Matrix:
         h = C.c_void_p()
         check(lib().gbk_mxm(C.byref(h), self.h, B.h, SEMIRING[semiring], stream_ptr(stream)), "gbk_mxm")
         return Matrix._adopt(h)
+
+    def triangle_count(self, stream=None) -> int:
+        """Burkhardt's sum((A*A) .* A) / 6 (oriented count on a symmetric loop-free A)."""
+        c = C.c_uint64(0)
+        check(lib().gbk_triangle_count(self.h, C.byref(c), stream_ptr(stream)), "gbk_triangle_count")
+        return int(c.value)
 
     def select(self, op: str, thunk=0.0, stream=None) -> "Matrix":
         """Matrix select (select.h:363-395): same structure, values kept where op keeps them, else 0."""

@@ -173,6 +173,14 @@ int gbk_mxm_masked(gbk_matrix* out, gbk_matrix M, gbk_matrix A, gbk_matrix B, gb
  * plus-times, plus-second, plus-one, min-plus, min-second, or-and. */
 int gbk_mxm(gbk_matrix* out, gbk_matrix A, gbk_matrix B, gbk_semiring sr, void* stream);
 
+/* Triangle count with Burkhardt's result, sum (sum ((A * A) .* A)) / 6
+ * (algorithms/tc/tc.hpp:209-217).  For a symmetric A without self loops
+ * (checked on the device against its CSC) each edge is oriented from its
+ * (degree, id)-smaller end and every triangle counted once by intersecting
+ * the oriented neighbour lists, which gives the same number; any other A
+ * takes the masked plus-one product as the formula stands. */
+int gbk_triangle_count(gbk_matrix A, uint64_t* count, void* stream);
+
 /* ---- select ---------------------------------------------------------------- */
 
 /* Index-unary operators of select: index ops keep a_ij by position (k = the
