@@ -65,17 +65,19 @@ def parse():
     p.add_argument("--seed", type=int, default=42)
     p.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--mode", default="spmv", choices=["spmv", "batched", "serve", "algorithms", "ingest"],
+    p.add_argument("--mode", default="spmv", choices=["spmv", "batched", "serve", "algorithms", "ingest", "spgemm"],
                    help="spmv: the SpMV line (default); batched: 64-source BFS + 32-column PPR / SSSP on "
                         "R-MAT s22; serve: Poisson request stream on a resident undirected R-MAT s24; "
                         "algorithms: BFS/CC/PR/SSSP/TC on undirected R-MAT s23 vs the reference CPU code; "
-                        "ingest: the R-MAT graph as .mtx / .mtxbin files into device CSR vs the reference reader")
+                        "ingest: the R-MAT graph as .mtx / .mtxbin files into device CSR vs the reference reader; "
+                        "spgemm: unmasked A*A and triangle counting on undirected R-MAT vs the reference")
     p.add_argument("--queries", type=int, default=1000, help="serve: requests in the trace")
     p.add_argument("--rate", type=float, default=2000.0, help="serve: mean arrival rate (queries/s)")
     p.add_argument("--serial-queries", type=int, default=60, help="serve: requests run one at a time")
     p.add_argument("--serve-scale", type=int, default=24, help="serve: R-MAT scale of the resident graph")
     p.add_argument("--alg-scale", type=int, default=23, help="algorithms: R-MAT scale")
     p.add_argument("--ingest-reps", type=int, default=3, help="ingest: timed reads per file")
+    p.add_argument("--spgemm-scale", type=int, default=15, help="spgemm: R-MAT scale (undirected)")
     p.add_argument("--no-extras", action="store_true",
                    help="default line without the batched / served summaries (SpMV only)")
     return p.parse_args()
@@ -866,6 +868,69 @@ def run_ingest(args):
     return out
 
 
+def run_spgemm(args):
+    """Sparse products on undirected R-MAT (--spgemm-scale): unmasked A (+.x) A (SpMSpM_unmasked_ikj), the
+    masked plus-one product C<A> = A A of Burkhardt's triangle count (SpMSpM_masked_ikj), and the triangle
+    count itself, each against the reference CPU code on the same graph (second of two runs timed)."""
+    import torch
+    from gb_kun_b200 import capi, graphgen as gg
+    capi.init(0)
+    g = gg.rmat(args.spgemm_scale, args.edge_factor, seed=args.seed, undirected=True)
+    val = gg.values_f32(g, seed=args.seed + 5)
+    A = capi.Matrix.from_graph(g, val)
+    Ai = capi.Matrix.from_graph(g, np.ones(g.nnz, np.int32))
+    R = _ref_threads()
+
+    def timed(fn):
+        out = fn()
+        if hasattr(out, "close"):
+            out.close()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return out, (time.perf_counter() - t0) * 1e3
+
+    deg = np.diff(g.row_ptr).astype(np.int64)
+    products = int(deg[g.col].sum())
+    C, mxm_ms = timed(lambda: A.mxm(A))
+    res = {"mxm_unmasked": {"gpu_ms": round(mxm_ms, 3), "products": products, "nnz_c": C.nnz,
+                            "G_products_per_s": round(products / (mxm_ms * 1e-3) / 1e9, 3)}}
+    if R is not None:
+        rp, col, v = C.download_csr()
+        rrp, rcol, rv, ref_ms = R.mxm(g, val, 0)
+        rows = np.repeat(np.arange(g.n), np.diff(rrp))
+        o = np.lexsort((rcol, rows))
+        res["mxm_unmasked"].update({"ref_cpu_ms": round(ref_ms, 1), "speedup": round(ref_ms / mxm_ms, 1),
+                                    "matches_reference": bool(np.array_equal(rp, rrp) and np.array_equal(col, rcol[o])
+                                                              and np.allclose(v, rv[o], rtol=2e-6))})
+    C.close()
+    tri, tc_ms = timed(lambda: Ai.triangle_count())
+    res["triangle_count"] = {"gpu_ms": round(tc_ms, 3), "triangles": tri}
+    from gb_kun_b200 import lablas_capi as lc
+    G = lc.Graph(g)
+    mtri, mtc_ms = timed(lambda: G.tc_method(2)[0])  # Cohen: select + masked plus-one product
+    res["triangle_count_masked_product"] = {"gpu_ms": round(mtc_ms, 3), "triangles": mtri}
+    if R is not None:
+        rtri, rms = R.tc(g)
+        res["triangle_count"].update({"ref_cpu_ms": round(rms, 1), "speedup": round(rms / tc_ms, 1),
+                                      "matches_reference": rtri == tri})
+        res["triangle_count_masked_product"]["matches_reference"] = rtri == mtri
+    out = {
+        "metric": "sparse products: unmasked A*A G products/s; triangle count vs the reference CPU code",
+        "value": res["mxm_unmasked"]["G_products_per_s"], "unit": "G products/s", "n_gpus": 1, "steps": 1,
+        "warmup": 1, "ms_per_step": res["mxm_unmasked"]["gpu_ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 / i32", "data": "synthetic (seeded R-MAT, generated in-process)",
+        "config": {"workload": f"spgemm_rmat{args.spgemm_scale}u", "n": g.n, "nnz": g.nnz,
+                   "timing": "host timer around each call (device synchronised), second of two runs"},
+        "products": res,
+        "cpu_baseline": None if R is None else {"value": res["mxm_unmasked"].get("ref_cpu_ms"), "unit": "ms (A*A)",
+                                                "cores": R.max_threads(), "kind": "reference",
+                                                "sample": "one unmasked mxm and one LAGr_TriangleCount"},
+    }
+    return out
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -900,7 +965,7 @@ def main():
     args = parse()
     if args.mode != "spmv":
         out = {"batched": run_batched, "serve": run_serve, "algorithms": run_algorithms,
-               "ingest": run_ingest}[args.mode](args)
+               "ingest": run_ingest, "spgemm": run_spgemm}[args.mode](args)
         print(json.dumps(out), flush=True)
     elif args.impl == "reference":
         run_reference(args)
