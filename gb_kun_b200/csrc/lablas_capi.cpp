@@ -37,6 +37,20 @@ struct Graph {
         if (!Af) Af = make<float>(std::vector<float>(col.size(), 1.0f));
         return Af.get();
     }
+    // The unit matrix with the storage format the autotuner picks for its
+    // unmasked plus-second SpMV (PageRank's product), tuned once per graph;
+    // masked and sparse products keep using the CSR / CSC views.
+    bool tuned_pr = false;
+    lablas::Matrix<float>* pagerank_matrix() {
+        auto* A = unit_f();
+        if (!tuned_pr) {
+            gbk_tune_result r;
+            lablas::throw_if(gbk_matrix_autotune(A->handle(), 0, GBK_PLUS_SECOND, 10, &r, lablas::stream()),
+                             "PageRank format autotune");
+            tuned_pr = true;
+        }
+        return A;
+    }
     lablas::Matrix<int>* unit_i() {
         if (!Ai) Ai = make<int>(std::vector<int>(col.size(), 1));
         return Ai.get();
@@ -197,7 +211,7 @@ int gbk_lablas_pagerank(gbk_lablas_graph g, int32_t itermax, double damping, dou
                         int32_t* iterations, double* ms) {
     if (!g || !ranks) return GBK_NULL_POINTER;
     return guarded([&] {
-        auto* A = g->unit_f();
+        auto* A = g->pagerank_matrix();
         LAGraph_Graph<float> graph(*A);
         lablas::Vector<float> r(g->n);
         int iters = 0;
@@ -215,7 +229,7 @@ int gbk_lablas_ppr(gbk_lablas_graph g, int64_t seed, int32_t itermax, double dam
     if (!g || !ranks) return GBK_NULL_POINTER;
     if (seed < 0 || seed >= g->n) return GBK_INVALID_INDEX;
     return guarded([&] {
-        auto* A = g->unit_f();
+        auto* A = g->pagerank_matrix();
         LAGraph_Graph<float> graph(*A);
         lablas::Vector<float> r(g->n);
         int iters = 0;
