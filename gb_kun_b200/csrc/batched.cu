@@ -774,84 +774,131 @@ struct PprState {
 };
 
 // The SpMM leaves each non-empty row's sum for the active lanes in r_out;
-// k_ppr_update turns it into the new rank.
-__device__ __forceinline__ void ppr_store_sum(float* r_out, int64_t row, float acc, bool mine) {
-    if (mine) __stcs(r_out + row * 32 + (threadIdx.x & 31), acc);
+// k_ppr_update turns it into the new rank.  Lane q of a quarter-warp holds
+// columns 4q .. 4q + 3; only the active ones are stored.
+__device__ __forceinline__ void ppr_store_sum4(float* r_out, int64_t row, float4 s, unsigned m4, int q) {
+    float* p = r_out + row * 32 + 4 * q;
+    if (m4 == 0xFu) {
+        __stcs(reinterpret_cast<float4*>(p), s);
+        return;
+    }
+    if (m4 & 1u) __stcs(p, s.x);
+    if (m4 & 2u) __stcs(p + 1, s.y);
+    if (m4 & 4u) __stcs(p + 2, s.z);
+    if (m4 & 8u) __stcs(p + 3, s.w);
 }
 
+__device__ __forceinline__ float4 ld_keep4(const float* p, uint64_t pol) {
+    float4 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p), "l"(pol));
+    return v;
+}
 
-// Gathers of w rows each warp keeps in flight (latency x bandwidth needs
-// tens of KB per SM outstanding).
-constexpr int kPprInFlight = 8;
+__device__ __forceinline__ float4 add4(float4 a, float4 b) {
+    return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
 
-// One warp per work item, lane k = column k.  An item is either a run of up
-// to 32 consecutive short rows or one piece of a long row; the warp loads 32
-// column ids at a time and keeps kPprInFlight gathers of 128-byte w rows in flight
-// whatever the row lengths, closing each row when the edge index passes its
-// end (rows are summed in CSR order, as the reference's loop does).  Lanes of
-// inactive columns issue no loads.  Pieces of split rows park their sums for
-// k_ppr_fix.
-__global__ void __launch_bounds__(kBT) k_ppr_spmm(const ColCfg* __restrict__ cfg, const PprState* __restrict__ st) {
+// (quarter 0 + quarter 1) + (quarter 2 + quarter 3), on every lane: float
+// addition commutes, so all four quarters end with the same bits.
+__device__ __forceinline__ float4 quarter_sum4(float4 a) {
+#pragma unroll
+    for (int o = 8; o < 32; o <<= 1) {
+        a.x += __shfl_xor_sync(kFull, a.x, o);
+        a.y += __shfl_xor_sync(kFull, a.y, o);
+        a.z += __shfl_xor_sync(kFull, a.z, o);
+        a.w += __shfl_xor_sync(kFull, a.w, o);
+    }
+    return a;
+}
+
+// 4-edge blocks each warp keeps in flight: 16 gathered 128-byte w rows.
+constexpr int kPprBlocks = 4;
+
+// One warp per work item.  An item is either a run of up to 32 consecutive
+// short rows or one piece of a long row.  The warp loads 32 column ids at a
+// time and works on 4 edges at once: quarter g (lanes 8g .. 8g + 7) gathers
+// the 128-byte w row of the item's edges g, g + 4, g + 8, ... as one 16-byte
+// load per lane (lane q: columns 4q .. 4q + 3).  Each quarter sums its edges of
+// a row in CSR order; when the edge index passes the row's end the quarters'
+// sums are added in a fixed order and stored.  The order of every column's
+// sum depends on the graph and the item cut only, never on which other
+// columns are active.  Lanes whose four columns are all inactive issue no
+// loads.  Pieces of split rows park their sums for k_ppr_fix.
+__global__ void __launch_bounds__(kBT, 4) k_ppr_spmm(const ColCfg* __restrict__ cfg, const PprState* __restrict__ st) {
     const unsigned act = (unsigned)st->st.active;
-    const int lane = threadIdx.x & 31;
+    if (!act) return;
+    const int lane = threadIdx.x & 31, g = lane >> 3, q = lane & 7;
+    const unsigned m4 = (act >> (4 * q)) & 0xFu;
+    const bool any = m4 != 0;
     const int cur = st->st.iter & 1;
-    const float* __restrict__ w_in = cfg->w[cur];
+    const float* __restrict__ w_q = cfg->w[cur] + 4 * q;
     float* r_out = cfg->r[cur ^ 1];
-    const bool mine = (act >> lane) & 1;
     const int32_t* __restrict__ rp = cfg->rp;
     const int32_t* __restrict__ col = cfg->col;
     const uint64_t pol = policy_evict_last();
-    const float* w_lane = w_in + lane;
-    if (act) {
-        const int64_t nitems = cfg->nitems;
-        const int64_t gw = ((int64_t)blockIdx.x * kBT + threadIdx.x) >> 5;
-        const int64_t nw = ((int64_t)gridDim.x * kBT) >> 5;
-        for (int64_t it = gw; it < nitems; it += nw) {
-            int32_t row = cfg->item_row[it];
-            const int32_t row_end = cfg->item_end[it];
-            const int32_t eb = cfg->item_beg[it], ee = cfg->item_ee[it];
-            const int32_t slot = cfg->item_slot[it];
-            int32_t bound = slot >= 0 ? ee : rp[row + 1];
-            float acc = 0.f;
-            for (int32_t e0 = eb; e0 < ee; e0 += 32) {
-                const int cnt = min(32, ee - e0);
-                const int32_t cl = lane < cnt ? __ldcs(col + e0 + lane) : 0;
-                for (int j = 0; j < cnt; j += kPprInFlight) {
-                    float t[kPprInFlight];
+    const int64_t nitems = cfg->nitems;
+    const int64_t gw = ((int64_t)blockIdx.x * kBT + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * kBT) >> 5;
+    for (int64_t it = gw; it < nitems; it += nw) {
+        int32_t row = cfg->item_row[it];
+        const int32_t row_end = cfg->item_end[it];
+        const int32_t eb = cfg->item_beg[it], ee = cfg->item_ee[it];
+        const int32_t slot = cfg->item_slot[it];
+        int32_t bound = slot >= 0 ? ee : rp[row + 1];
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int32_t e0 = eb; e0 < ee; e0 += 32) {
+            const int cnt = min(32, ee - e0);
+            const int32_t cl = lane < cnt ? __ldcs(col + e0 + lane) : 0;
+            for (int j = 0; j < cnt; j += 4 * kPprBlocks) {
+                float4 t[kPprBlocks];
 #pragma unroll
-                    for (int q = 0; q < kPprInFlight; ++q) {
-                        const int32_t u = __shfl_sync(kFull, cl, (j + q) & 31);
-                        t[q] = (mine && j + q < cnt) ? ld_keep(w_lane + ((int64_t)u << 5), pol) : 0.f;
-                    }
-                    // whole block inside the current row: plain adds (the
-                    // padding entries are +0, which leaves the sum unchanged)
-                    if (e0 + min(j + kPprInFlight, cnt) <= bound) {
+                for (int b = 0; b < kPprBlocks; ++b) {
+                    const int k = j + 4 * b + g;
+                    const int32_t u = __shfl_sync(kFull, cl, k & 31);
+                    t[b] = (any && k < cnt) ? ld_keep4(w_q + ((int64_t)u << 5), pol) : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                // all these edges inside the current row: plain adds (edges
+                // past cnt were loaded as +0, which leaves the sums unchanged)
+                if (e0 + min(j + 4 * kPprBlocks, cnt) <= bound) {
 #pragma unroll
-                        for (int q = 0; q < kPprInFlight; ++q) acc += t[q];
-                        continue;
-                    }
+                    for (int b = 0; b < kPprBlocks; ++b) acc = add4(acc, t[b]);
+                    continue;
+                }
 #pragma unroll
-                    for (int q = 0; q < kPprInFlight; ++q) {
-                        if (j + q < cnt) {
-                            const int32_t e = e0 + j + q;
-                            while (e >= bound) {  // rows that end here (empty rows need no store)
-                                if (bound > rp[row]) ppr_store_sum(r_out, row, acc, mine);
-                                acc = 0.f;
-                                ++row;
-                                bound = rp[row + 1];
-                            }
-                            acc += t[q];
+                for (int b = 0; b < kPprBlocks; ++b) {
+                    const int nb = min(4, cnt - (j + 4 * b));  // edges of this block (warp-uniform)
+                    if (nb <= 0) break;
+                    const int32_t base = e0 + j + 4 * b;
+                    bool pending = g < nb;
+                    while (base + nb > bound) {  // rows that end inside this block (empty rows need no store)
+                        if (pending && base + g < bound) {
+                            acc = add4(acc, t[b]);
+                            pending = false;
                         }
+                        const float4 s = quarter_sum4(acc);
+                        if (g == 0 && bound > rp[row]) ppr_store_sum4(r_out, row, s, m4, q);
+                        acc = make_float4(0.f, 0.f, 0.f, 0.f);
+                        ++row;
+                        bound = rp[row + 1];
                     }
+                    if (pending) acc = add4(acc, t[b]);
                 }
             }
-            if (slot >= 0) {
-                cfg->split_acc[(int64_t)slot * 32 + lane] = acc;
-                continue;
-            }
-            if (row < row_end && rp[row + 1] > rp[row]) ppr_store_sum(r_out, row, acc, mine);
         }
+        const float4 s = quarter_sum4(acc);
+        if (slot >= 0) {
+            if (g == 0) *reinterpret_cast<float4*>(cfg->split_acc + (int64_t)slot * 32 + 4 * q) = s;
+            continue;
+        }
+        if (g == 0 && row < row_end && rp[row + 1] > rp[row]) ppr_store_sum4(r_out, row, s, m4, q);
     }
+}
+
+// Lane k stores column k of a split row's sum.
+__device__ __forceinline__ void ppr_store_sum(float* r_out, int64_t row, float acc, bool mine) {
+    if (mine) __stcs(r_out + row * 32 + (threadIdx.x & 31), acc);
 }
 
 __global__ void __launch_bounds__(kBT) k_ppr_fix(const ColCfg* __restrict__ cfg, const PprState* __restrict__ st) {
@@ -881,7 +928,7 @@ __global__ void __launch_bounds__(kBT) k_ppr_fix(const ColCfg* __restrict__ cfg,
 // the teleport at the seed, w = rank / d, and the per-column partial sums of
 // |rank - old| and of the rank held by sinks, per block in a fixed order.
 // Inactive columns are written back unchanged.
-__global__ void __launch_bounds__(kBT) k_ppr_update(const ColCfg* __restrict__ cfg, const PprState* __restrict__ st) {
+__global__ void __launch_bounds__(kBT, 3) k_ppr_update(const ColCfg* __restrict__ cfg, const PprState* __restrict__ st) {
     __shared__ double s_sink[kBT / 32][32], s_rd[kBT / 32][32];
     const unsigned act = (unsigned)st->st.active;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, quad = threadIdx.x & 7;
