@@ -843,10 +843,14 @@ __global__ void __launch_bounds__(kBT, 4) k_ppr_spmm(const ColCfg* __restrict__ 
     const int64_t nw = ((int64_t)gridDim.x * kBT) >> 5;
     for (int64_t it = gw; it < nitems; it += nw) {
         int32_t row = cfg->item_row[it];
-        const int32_t row_end = cfg->item_end[it];
+        const int32_t row0 = row, row_end = cfg->item_end[it];
         const int32_t eb = cfg->item_beg[it], ee = cfg->item_ee[it];
         const int32_t slot = cfg->item_slot[it];
-        int32_t bound = slot >= 0 ? ee : rp[row + 1];
+        // the ends of the item's rows (at most 32), one per lane: row r ends
+        // at lane r - row0's value (a split piece ends at its own end)
+        const int32_t rpl = (slot < 0 && row0 + 1 + lane <= row_end) ? rp[row0 + 1 + lane] : ee;
+        int32_t bound = __shfl_sync(kFull, rpl, 0);
+        int32_t start = eb;  // where the current row begins
         float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
         for (int32_t e0 = eb; e0 < ee; e0 += 32) {
             const int cnt = min(32, ee - e0);
@@ -878,10 +882,11 @@ __global__ void __launch_bounds__(kBT, 4) k_ppr_spmm(const ColCfg* __restrict__ 
                             pending = false;
                         }
                         const float4 s = quarter_sum4(acc);
-                        if (g == 0 && bound > rp[row]) ppr_store_sum4(r_out, row, s, m4, q);
+                        if (g == 0 && bound > start) ppr_store_sum4(r_out, row, s, m4, q);
                         acc = make_float4(0.f, 0.f, 0.f, 0.f);
+                        start = bound;
                         ++row;
-                        bound = rp[row + 1];
+                        bound = __shfl_sync(kFull, rpl, (row - row0) & 31);
                     }
                     if (pending) acc = add4(acc, t[b]);
                 }
@@ -892,7 +897,7 @@ __global__ void __launch_bounds__(kBT, 4) k_ppr_spmm(const ColCfg* __restrict__ 
             if (g == 0) *reinterpret_cast<float4*>(cfg->split_acc + (int64_t)slot * 32 + 4 * q) = s;
             continue;
         }
-        if (g == 0 && row < row_end && rp[row + 1] > rp[row]) ppr_store_sum4(r_out, row, s, m4, q);
+        if (g == 0 && row < row_end && bound > start) ppr_store_sum4(r_out, row, s, m4, q);
     }
 }
 
