@@ -40,6 +40,9 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
 
 int num_sms();
 void count_launch(int n);
+// Loads the allocation-free conversion's module and caches its scratch
+// address for `device` (current); noalloc.cu.
+int noalloc_setup(int device);
 
 // Every kernel launch site calls this once the launch is issued.
 #define GBK_LAUNCHED()                \

@@ -78,7 +78,9 @@ int gbk_init(int device) {
     GBK_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
     uint64_t keep = UINT64_MAX;
     GBK_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-    return GBK_SUCCESS;
+    // Load the allocation-free entry point's code and scratch now, while
+    // memory is free, instead of on its first call.
+    return gbk::noalloc_setup(device);
 }
 
 int gbk_get_last_error(char* buf, size_t len) {

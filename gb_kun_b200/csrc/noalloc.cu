@@ -17,9 +17,20 @@
 // All calls share it and every slot a call reads is written earlier in the
 // same call (nothing has to start at zero); calls that overlap on the GPU
 // (different streams, or different host threads without ordering) race on
-// it.  The first call on each device looks up the array's device address
-// (cudaGetSymbolAddress, no allocation); make that first call before any
-// stream capture begins.
+// it.
+//
+// Set-up: CUDA loads a module's code and its __device__ arrays lazily, on
+// first use, and that load allocates device memory.  gbk_init therefore runs
+// noalloc_setup for its device: it looks up the array's device address
+// (cudaGetSymbolAddress, with the device current) and queries the three
+// kernels (cudaFuncGetAttributes), which loads them, so the array and the
+// code are resident before any caller runs out of memory.  The address is
+// cached per device.  A device that never saw gbk_init gets the same set-up
+// on its first call here; make that first call before any stream capture.
+// After cudaDeviceReset the module is loaded again and may move: call
+// gbk_init again, which refreshes the cached address.
+#include <atomic>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -141,22 +152,44 @@ __global__ void __launch_bounds__(kNoAllocThreads) k_na_write(const void* v, int
     }
 }
 
-// Device address of the scratch array, looked up once per device.
-int scratch_address(int32_t** out) {
-    static int32_t* addr[64] = {nullptr};
-    int dev = 0;
-    GBK_CUDA(cudaGetDevice(&dev));
-    GBK_REQUIRE(dev >= 0 && dev < 64, GBK_INVALID_VALUE, "gbk_vec_to_sparse_noalloc: device id %d", dev);
-    if (!addr[dev]) {
-        void* p = nullptr;
-        GBK_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        addr[dev] = (int32_t*)p;
-    }
-    *out = addr[dev];
+constexpr int kNoAllocMaxDevices = 64;
+std::atomic<int32_t*> g_scratch_addr[kNoAllocMaxDevices];
+
+// Looks up the array's device address for the current device and loads the
+// kernels; stores the address in the per-device cache.
+int setup_current_device(int dev, int32_t** out) {
+    void* p = nullptr;
+    GBK_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    cudaFuncAttributes fa;
+    GBK_CUDA(cudaFuncGetAttributes(&fa, k_na_count));
+    GBK_CUDA(cudaFuncGetAttributes(&fa, k_na_offsets));
+    GBK_CUDA(cudaFuncGetAttributes(&fa, k_na_write));
+    g_scratch_addr[dev].store((int32_t*)p, std::memory_order_release);
+    if (out) *out = (int32_t*)p;
     return GBK_SUCCESS;
 }
 
+// Device address of the scratch array for the current device.
+int scratch_address(int32_t** out) {
+    int dev = 0;
+    GBK_CUDA(cudaGetDevice(&dev));
+    GBK_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, GBK_INVALID_VALUE, "gbk_vec_to_sparse_noalloc: device id %d",
+                dev);
+    int32_t* a = g_scratch_addr[dev].load(std::memory_order_acquire);
+    if (a) {
+        *out = a;
+        return GBK_SUCCESS;
+    }
+    return setup_current_device(dev, out);  // two threads racing here store the same address
+}
+
 }  // namespace
+
+// Called by gbk_init with `device` current.
+int noalloc_setup(int device) {
+    GBK_REQUIRE(device >= 0 && device < kNoAllocMaxDevices, GBK_INVALID_VALUE, "gbk_init: device id %d", device);
+    return setup_current_device(device, nullptr);
+}
 
 }  // namespace gbk
 
@@ -172,7 +205,7 @@ extern "C" int gbk_vec_to_sparse_noalloc(const void* dense, gbk_dtype t, int64_t
     GBK_REQUIRE(dtype_size(t) > 0, GBK_INVALID_VALUE, "gbk_vec_to_sparse_noalloc: bad type %d", (int)t);
     cudaStream_t s = (cudaStream_t)stream;
     int32_t* scratch = nullptr;
-    int rc = scratch_address(&scratch);  // first call on a device: symbol lookup, no allocation
+    int rc = scratch_address(&scratch);  // cached by gbk_init, else set up here
     if (rc) return rc;
     if (n == 0) {
         *nvals = 0;

@@ -376,6 +376,8 @@ int gbk_vec_to_sparse(const void* dense, gbk_dtype t, int64_t n, int32_t* ids, v
         return GBK_SUCCESS;
     }
     GBK_REQUIRE(dense && ids && vals, GBK_NULL_POINTER, "gbk_vec_to_sparse: NULL array");
+    GBK_REQUIRE(n > 0 && n < INT32_MAX, GBK_INVALID_VALUE, "gbk_vec_to_sparse: n = %lld outside [0, 2^31 - 1)",
+                (long long)n);
     int32_t *flag = nullptr, *pos = nullptr;
     GBK_CUDA(cudaMallocAsync((void**)&flag, sizeof(int32_t) * (n + 1), s));
     GBK_CUDA(cudaMallocAsync((void**)&pos, sizeof(int32_t) * (n + 1), s));

@@ -277,9 +277,12 @@ int gbk_vec_to_sparse(const void* dense, gbk_dtype t, int64_t n, int32_t* ids, v
  * application that budgets device memory up front.  Its scratch is a fixed
  * ~32 KiB array inside the library, held on every GPU that loads it until
  * exit, so n is limited to 33,554,432 (larger n: GBK_INVALID_VALUE).  All
- * calls share the scratch: calls that overlap on the GPU race.  The first
- * call on each device looks up the scratch address; make it before any
- * stream capture begins.  Synchronises the stream. */
+ * calls share the scratch: calls that overlap on the GPU race.  gbk_init
+ * loads this entry point's code and scratch on its device and caches the
+ * scratch address, so the calls themselves allocate nothing; on a device
+ * that never saw gbk_init the first call does that set-up (which may
+ * allocate), so make it before any stream capture begins.  After
+ * cudaDeviceReset call gbk_init again.  Synchronises the stream. */
 int gbk_vec_to_sparse_noalloc(const void* dense, gbk_dtype t, int64_t n, int32_t* ids, void* vals,
                               int64_t* nvals, void* stream);
 /* Sparse -> dense: zero fill, then scatter (DenseVector::convert, dense_vector.hpp:87-102). */

@@ -50,7 +50,32 @@ def make(n, density, dtype, seed):
     return torch.from_numpy(x.astype(dtype)).cuda()
 
 
-@pytest.mark.parametrize("dtype", [np.float32, np.int32, np.int64])
+def pool_state():
+    """Reserved and high-water bytes of the device's default stream-ordered
+    pool and the device's free memory, read through the CUDA runtime."""
+    rt = C.CDLL("libcudart.so.12") if _has("libcudart.so.12") else C.CDLL("libcudart.so")
+    dev = C.c_int()
+    assert rt.cudaGetDevice(C.byref(dev)) == 0
+    pool = C.c_void_p()
+    assert rt.cudaDeviceGetDefaultMemPool(C.byref(pool), dev) == 0
+    out = []
+    for attr in (5, 8):  # cudaMemPoolAttrReservedMemCurrent, cudaMemPoolAttrUsedMemHigh
+        v = C.c_uint64()
+        assert rt.cudaMemPoolGetAttribute(pool, attr, C.byref(v)) == 0
+        out.append(v.value)
+    free, _ = torch.cuda.mem_get_info()
+    return out[0], out[1], free
+
+
+def _has(name):
+    try:
+        C.CDLL(name)
+        return True
+    except OSError:
+        return False
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.int32, np.int64, np.float64, np.bool_])
 def test_matches_allocating_conversion_twice(capi, dtype):
     # first call: dense vector; second call: a sparser one, so stale scratch would show
     for n, dens, seed in [(3_000_001, 0.4, 1), (1_234_567, 0.001, 2)]:
@@ -60,6 +85,28 @@ def test_matches_allocating_conversion_twice(capi, dtype):
         assert ids.numel() == ref_ids.numel()
         assert torch.equal(ids, ref_ids)
         assert torch.equal(vals, ref_vals)
+
+
+def test_calls_allocate_nothing(capi):
+    # inputs and outputs are allocated first; then repeated calls must leave the
+    # stream-ordered pool and the device's free memory exactly as they were
+    d = make(2_000_003, 0.3, np.float32, 9)
+    n = d.numel()
+    ids = torch.empty(n, dtype=torch.int32, device="cuda")
+    vals = torch.empty(n, dtype=torch.float32, device="cuda")
+    nv = C.c_int64(-1)
+    fn = capi.lib().gbk_vec_to_sparse_noalloc
+    args = (capi.ptr(d), capi.dtype_code(d), n, capi.ptr(ids), capi.ptr(vals), C.byref(nv), capi.stream_ptr())
+    capi.check(fn(*args), "gbk_vec_to_sparse_noalloc")
+    torch.cuda.synchronize()
+    before = pool_state()
+    for _ in range(5):
+        capi.check(fn(*args), "gbk_vec_to_sparse_noalloc")
+    torch.cuda.synchronize()
+    after = pool_state()
+    assert before == after
+    ref_ids, _ = capi.to_sparse(d)
+    assert nv.value == ref_ids.numel()
 
 
 def test_edge_sizes_and_limit(capi):
