@@ -4,6 +4,8 @@
 * ``gb_kun_b200/libgbk_graphgen.so``  seeded graph generator (g++ / OpenMP)
 * ``gb_kun_b200/libgbk_lablas.so``    C++ lablas:: API + algorithms over the C ABI
 * ``oracle/liboracle.so`` and ``oracle/_ref/*``  CPU checkers (test infrastructure)
+* ``tests/dropin/_bin/ref_algorithms``  the reference's algorithm files on the
+  drop-in header (test infrastructure)
 
 Run ``python -m gb_kun_b200.build`` or call :func:`build_all`.
 """
@@ -34,6 +36,7 @@ CU_SOURCES = [
     "spmv_formats.cu",
     "spmv_segsmem.cu",
     "spmspv.cu",
+    "spmspv_sparse.cu",
     "vector_ops.cu",
     "spgemm.cu",
     "tune.cu",
@@ -127,11 +130,33 @@ def build_oracle(force=False) -> None:
     the reference sources are present (never on a machine without them)."""
     env = dict(os.environ)
     targets = [str(ROOT / "oracle" / "liboracle.so")]
-    ref_dir = Path(env.get("GBK_REF_DIR", "/root/reference"))
+    # the reference checkout: GBK_REF_DIR, else a "reference" directory beside the repository
+    ref_dir = Path(env.get("GBK_REF_DIR", str(ROOT.parent / "reference")))
+    env["GBK_REF_DIR"] = str(ref_dir)
     if (ref_dir / "src" / "gb_kun.h").exists():
         targets.append("ref")
     cmd = ["make", "-C", str(ROOT / "oracle")] + (["-B"] if force else []) + targets
-    _run(cmd)
+    res = subprocess.run(cmd, capture_output=True, text=True, env=env)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError(f"build step failed: {' '.join(cmd)}")
+
+
+def build_dropin(force=False) -> None:
+    """tests/dropin/_bin/ref_algorithms: the reference's own algorithm files,
+    unmodified, compiled against the drop-in header (gb_kun_b200/dropin/src)
+    and linked with libgbk.so; test infrastructure, built only where the
+    reference sources are present."""
+    env = dict(os.environ)
+    ref_dir = Path(env.get("GBK_REF_DIR", str(ROOT.parent / "reference")))
+    if not (ref_dir / "algorithms" / "bfs" / "bfs.hpp").exists():
+        return
+    env["GBK_REF_DIR"] = str(ref_dir)
+    cmd = ["make", "-C", str(ROOT / "tests" / "dropin")] + (["-B"] if force else [])
+    res = subprocess.run(cmd, capture_output=True, text=True, env=env)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError(f"build step failed: {' '.join(cmd)}")
 
 
 def build_all(force=False, verbose=False) -> None:
@@ -139,6 +164,7 @@ def build_all(force=False, verbose=False) -> None:
     build_core(force, verbose)
     build_lablas(force)
     build_oracle(force)
+    build_dropin(force)
 
 
 if __name__ == "__main__":

@@ -105,6 +105,7 @@ def _declare(lib):
     sig = {
         "gbk_mxv_sparse_mask": ([vp, ci, ci, ci, ci, vp, vp, vp, i64, ci, vp], ci),
         "gbk_spmspv": ([vp, ci, ci, ci, ci, vp, vp, i64, vp, mp, vp], ci),
+        "gbk_spmspv_sparse": ([vp, ci, ci, ci, vp, vp, i64, vp, vp, C.POINTER(i64), mp, vp], ci),
         "gbk_mxm_masked": ([C.POINTER(vp), vp, vp, vp, ci, ci, vp], ci),
         "gbk_matrix_autotune": ([vp, ci, ci, i32, C.POINTER(TuneResult), vp], ci),
         "gbk_vec_nvals": ([vp, ci, i64, C.POINTER(i64), vp], ci),
@@ -358,6 +359,18 @@ class Matrix:
                                ptr(x_vals), int(x_ids.numel()), ptr(y), C.byref(mask) if mask is not None else None,
                                stream_ptr(stream)), "gbk_spmspv")
         return y
+
+    def spmspv_sparse(self, x_ids, x_vals, semiring="lor_land", transpose=False, stream=None):
+        """Push SpMSpV with a sparse output: (ids ascending, values) of every reached row."""
+        import torch
+        n = self.info().ncols if transpose else self.info().nrows
+        y_ids = torch.empty(max(n, 1), dtype=torch.int32, device=x_vals.device)
+        y_vals = torch.empty(max(n, 1), dtype=x_vals.dtype, device=x_vals.device)
+        nv = C.c_int64()
+        check(lib().gbk_spmspv_sparse(self.h, int(transpose), SEMIRING[semiring], dtype_code(x_vals), ptr(x_ids),
+                                      ptr(x_vals), int(x_ids.numel()), ptr(y_ids), ptr(y_vals), C.byref(nv), None,
+                                      stream_ptr(stream)), "gbk_spmspv_sparse")
+        return y_ids[:nv.value], y_vals[:nv.value]
 
     def msbfs(self, sources, levels, direction=0, stream=None):
         """BFS levels from up to 64 sources at once into levels (device int32, len(sources) x n).

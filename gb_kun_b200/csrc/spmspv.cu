@@ -6,10 +6,16 @@
 // each OpenMP thread frontier vertices and updates y with `omp atomic`,
 // plain stores or an `omp critical` section per edge.  Here the work unit is
 // an edge: a scan of the frontier degrees turns the frontier into one flat
-// edge range, each thread takes kPushItems consecutive edges (one binary
-// search, then a forward walk), so a hub vertex is spread over many warps.
-// Updates are hardware atomics (add / min on integers, CAS loops on floats);
-// or-monoids store 1 without an atomic, as the reference does.
+// edge range, cut into warp tiles of 256 consecutive edges, so a hub vertex
+// is spread over many warps.  Per tile the warp finds the frontier entry of
+// the tile's first edge (a 32-way search, one load per lane per round); per
+// 32-edge sub-tile the lanes load the next 32 entry boundaries and each lane
+// finds its own entry by a 5-step search over those boundaries in registers
+// (shuffles).  Updates are warp-aggregated:
+// lanes whose edges hit the same output element (match-any on the index)
+// combine their values with the semiring's add in a tree over the group,
+// and one lane per group issues the atomic (add; min on integers, a CAS loop
+// on floats).  Or-monoids store 1 without an atomic, as the reference does.
 #include <cub/cub.cuh>
 
 #include "common.cuh"
@@ -33,21 +39,6 @@ __device__ __forceinline__ void atomic_min_val(float* p, float v) {
     }
 }
 
-template <int SR, typename T>
-__device__ __forceinline__ void push_update(int probe, T* y, int32_t j, T m) {
-    using S = Semiring<SR, T>;
-    if (probe == 8) {
-        atomicAdd(y + j, m);
-    } else if (probe == 1) {
-        y[j] = T(1);
-    } else if (SR == GBK_FIRST_WINS) {
-        // first(y, m) == y: the reference leaves y unchanged
-    } else {
-        // min-monoids (min, first-min, min-plus, min-second, min-noteq)
-        atomic_min_val(y + j, S::add(Lim<T>::max(), m));
-    }
-}
-
 __global__ void k_frontier_degrees(const int32_t* __restrict__ ptr, const int32_t* __restrict__ ids, int64_t nf,
                                    int32_t* __restrict__ deg) {
     int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -55,6 +46,51 @@ __global__ void k_frontier_degrees(const int32_t* __restrict__ ptr, const int32_
     if (k == nf) deg[k] = 0;
 }
 
+// Bit position of the r-th (0-based) set bit of m (m has more than r bits).
+__device__ __forceinline__ int nth_set_bit(unsigned m, int r) {
+    int pos = 0;
+#pragma unroll
+    for (int w = 16; w >= 1; w >>= 1)
+        if (__popc(m & ((1u << (pos + w)) - 1u)) <= r) pos += w;
+    return pos;
+}
+
+template <int SR, typename T>
+__device__ __forceinline__ void push_atomic(int probe, T* y, int32_t j, T v) {
+    using S = Semiring<SR, T>;
+    if (probe == 8)
+        atomicAdd(y + j, v);
+    else  // min-monoids (min, first-min, min-plus, min-second, min-noteq)
+        atomic_min_val(y + j, S::add(Lim<T>::max(), v));
+}
+
+// Largest k in [0, nf) with offs[k] <= e (offs ascending, offs[nf] > e),
+// found by the whole warp: each round the 31 lanes probe 31 evenly spaced
+// entries of the open range and a ballot keeps the sub-range, so a frontier
+// of n entries takes about log32(n) rounds of one load each.
+__device__ __forceinline__ int64_t warp_find_entry(const int32_t* __restrict__ offs, int64_t nf, int64_t e,
+                                                   int lane) {
+    int64_t lo = 0, hi = nf;  // offs[lo] <= e < offs[hi] (offs[nf] = E > e)
+    while (hi - lo > 1) {
+        const int64_t span = hi - lo;
+        const int64_t p = lo + (span * (lane + 1) + 31) / 32;  // lanes 0..30 probe inside (lo, hi]
+        const bool le = lane < 31 && p < hi && offs[p] <= e;
+        const unsigned bal = __ballot_sync(0xffffffffu, le);
+        const int c = __popc(bal);  // a prefix of the lanes (offs ascends)
+        const int64_t p_c = __shfl_sync(0xffffffffu, p, c < 31 ? c : 30);
+        const int64_t p_last = __shfl_sync(0xffffffffu, p, c > 0 ? c - 1 : 0);
+        if (c > 0) lo = p_last;
+        if (c < 31) hi = p_c;
+    }
+    return lo;
+}
+
+constexpr int kPushSubTiles = 8;  // 32-edge sub-tiles per warp tile
+
+// One warp per tile of 256 consecutive frontier edges (grid-stride over
+// tiles; the loops are warp-uniform, so every shuffle sees all 32 lanes).
+// The tile's first entry comes from one warp search; each 32-edge sub-tile
+// starts from the entry of the previous sub-tile's last edge.
 template <int SR, typename T>
 __global__ void __launch_bounds__(kPushThreads) k_push(const int32_t* __restrict__ ptr,
                                                        const int32_t* __restrict__ idx, const T* __restrict__ val,
@@ -62,28 +98,78 @@ __global__ void __launch_bounds__(kPushThreads) k_push(const int32_t* __restrict
                                                        int64_t nf, const int32_t* __restrict__ offs, int probe,
                                                        T* __restrict__ y) {
     using S = Semiring<SR, T>;
+    constexpr unsigned kFull = 0xffffffffu;
+    constexpr int64_t kTile = 32 * kPushSubTiles;
+    const int lane = threadIdx.x & 31;
     const int64_t E = offs[nf];
-    const int64_t chunks = (E + kPushItems - 1) / kPushItems;
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < chunks;
-         c += (int64_t)gridDim.x * blockDim.x) {
-        int64_t e = c * kPushItems;
-        // frontier entry owning edge e: largest k with offs[k] <= e
-        int64_t lo = 0, hi = nf;
-        while (hi - lo > 1) {
-            int64_t mid = (lo + hi) >> 1;
-            if (offs[mid] <= e)
-                lo = mid;
-            else
-                hi = mid;
-        }
-        int64_t k = lo;
-        const int64_t e_end = min(e + kPushItems, E);
-        for (; e < e_end; e++) {
-            while (offs[k + 1] <= e) k++;
-            const int32_t src = ids[k];
-            const int64_t pos = ptr[src] + (e - offs[k]);
-            const int32_t j = idx[pos];
-            push_update<SR, T>(probe, y, j, S::mul(val[pos], xv[k]));
+    const int64_t ntiles = (E + kTile - 1) / kTile;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; t < ntiles; t += nwarps) {
+        int64_t k0 = warp_find_entry(offs, nf, t * kTile, lane);
+        for (int sub = 0; sub < kPushSubTiles; ++sub) {
+            const int64_t e0 = t * kTile + 32 * sub;
+            if (e0 >= E) break;
+            const int32_t start0 = offs[k0];
+            // boundary of entry k0 + 1 + lane (E past the last entry)
+            const int64_t kb = k0 + 1 + lane;
+            const int32_t b = kb <= nf ? offs[kb] : (int32_t)E;
+            const int64_t e = e0 + lane;
+            const bool valid = e < E;
+            // cnt = boundaries <= e among the 32 (they ascend with the lane)
+            int cnt = 0;
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1) {
+                const int32_t bv = __shfl_sync(kFull, b, cnt + step - 1);
+                if (bv <= e) cnt += step;
+            }
+            const int32_t b31 = __shfl_sync(kFull, b, 31);
+            const int32_t prev = __shfl_sync(kFull, b, cnt > 0 ? cnt - 1 : 0);
+            int64_t k;
+            int32_t start;
+            if (valid && cnt == 31 && b31 <= e) {
+                // more than 32 entries end before this edge (empty rows): search on
+                int64_t lo = k0 + 32, hi = nf;
+                while (hi - lo > 1) {
+                    const int64_t mid = (lo + hi) >> 1;
+                    if (offs[mid] <= e)
+                        lo = mid;
+                    else
+                        hi = mid;
+                }
+                k = lo;
+                start = offs[k];
+            } else {
+                k = k0 + cnt;  // an entry of the frontier for every valid lane
+                start = cnt > 0 ? prev : start0;
+            }
+            int32_t j = -1 - lane;  // a key no other lane has
+            T m = S::identity();
+            if (valid) {
+                const int32_t src = ids[k];
+                const int64_t pos = ptr[src] + (e - start);
+                j = idx[pos];
+                m = S::mul(val[pos], xv[k]);
+            }
+            if (probe == 1) {
+                if (valid) y[j] = T(1);
+            } else if (SR != GBK_FIRST_WINS) {
+                // first(y, m) == y leaves y unchanged; every other add folds per group
+                const unsigned peers = __match_any_sync(kFull, j);
+                const int rank = __popc(peers & ((1u << lane) - 1u));
+                const int gsize = __popc(peers);
+                T acc = m;
+                for (int st = 1; st < 32; st <<= 1) {
+                    if (!__any_sync(kFull, gsize > st)) break;
+                    const bool take = (rank % (2 * st)) == 0 && rank + st < gsize;
+                    const int from = take ? nth_set_bit(peers, rank + st) : lane;
+                    const T o = __shfl_sync(kFull, acc, from);
+                    if (take) acc = S::add(acc, o);
+                }
+                if (valid && rank == 0) push_atomic<SR, T>(probe, y, j, acc);
+            }
+            // the next sub-tile starts in the entry of this one's last edge
+            // (valid whenever a next sub-tile exists: e0 + 32 < E)
+            k0 = __shfl_sync(kFull, k, 31);
         }
     }
 }

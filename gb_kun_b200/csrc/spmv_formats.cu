@@ -93,6 +93,8 @@ struct SegCsr {
     int32_t* col_new_to_old = nullptr;  // LAV only: x reorder
     void* xr = nullptr;                 // LAV only: reordered x (ncols)
     int64_t ncols = 0;
+    SegSmem* staged = nullptr;          // LAV only: the renumbered matrix in staged windows
+    int64_t dense_cols = 0;             // LAV only: renumbered columns holding the dense fraction of nnz
 };
 
 namespace {
@@ -477,6 +479,41 @@ __global__ void k_reorder_x(const T* __restrict__ x, const int32_t* __restrict__
     if (i < n) xr[i] = x[new_to_old[i]];
 }
 
+// LAV column renumbering on the device (lav/build.hpp:113-141): in-degree of
+// every column, columns sorted by it (descending, ties in column order: a
+// stable radix sort), the inverse map, and the stored column ids relabelled.
+// (k_col_hist and k_invert_perm, shared with the SELL-C renumbering, are
+// defined with the SELL-C build below.)
+__global__ void k_col_hist(const int32_t* __restrict__ idx, int64_t nnz, int32_t* __restrict__ cdeg);
+__global__ void k_invert_perm(const int32_t* new_to_old, int64_t n, int32_t* old_to_new);
+
+__global__ void k_iota32(int32_t* __restrict__ v, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) v[i] = (int32_t)i;
+}
+
+__global__ void k_relabel(const int32_t* __restrict__ idx, int64_t nnz, const int32_t* __restrict__ old_to_new,
+                          int32_t* __restrict__ out) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x)
+        out[e] = old_to_new[idx[e]];
+}
+
+// First renumbered column at which the running in-degree sum reaches
+// `target` (the reference's dense_threshold); one thread, binary search over
+// the inclusive scan of the sorted degrees.
+__global__ void k_dense_threshold(const long long* __restrict__ acc, int64_t n, long long target,
+                                  long long* __restrict__ out) {
+    int64_t lo = 0, hi = n;  // first c with acc[c] >= target, n if none
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (acc[mid] >= target)
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    *out = lo;
+}
+
 // Segment id of every entry: key = (segment << 32) | row, value = entry position.
 __global__ void k_seg_keys(const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx, int64_t nrows,
                            int64_t nnz, const int32_t* __restrict__ col_seg, unsigned long long* __restrict__ keys,
@@ -594,6 +631,7 @@ int free_seg(SegCsr* f) {
     cudaFree(f->partial);
     cudaFree(f->col_new_to_old);
     cudaFree(f->xr);
+    free_segsmem(f->staged);
     delete f;
     return 0;
 }
@@ -1019,9 +1057,96 @@ int build_seg(const CsrView& a, int32_t seg_cols, SegCsr** out, cudaStream_t s) 
     return GBK_SUCCESS;
 }
 
-// LAV (lav/build.hpp:97-212): columns renumbered by in-degree, descending;
-// the columns holding the first dense_frac of nnz form "dense" segments of
-// seg_cols columns, the rest one "sparse" segment.
+// LAV with staged windows: the reference's column order (in-degree,
+// descending; lav/build.hpp:113-141), computed on the device, and the
+// renumbered matrix in the staged-window layout of CSR_SEG.  The renumbering
+// packs the most used columns into the first windows -- the reference's
+// "dense" segments (the columns holding dense_frac of nnz, lav/build.hpp:
+// 143-160) -- so those windows are dense and each is staged once per CTA;
+// the reference's one "sparse" segment becomes the remaining windows, staged
+// the same way.  x is gathered into the new order on every call
+// (spmv_lav.h:24-26).
+int build_lav_staged(const CsrView& a, int dtype, float dense_frac, SegCsr** out, cudaStream_t s) {
+    const int64_t nc = a.ncols, nnz = a.nnz;
+    SegCsr* f = new SegCsr();
+    f->n = a.nrows;
+    f->ncols = nc;
+    const size_t eb = dtype == GBK_F32 ? sizeof(float) : sizeof(int32_t);
+    int32_t *cdeg = nullptr, *cdeg_sorted = nullptr, *iota = nullptr, *old_to_new = nullptr, *idx2 = nullptr;
+    long long *acc = nullptr, *thr = nullptr;
+    const int64_t nc1 = nc > 0 ? nc : 1;
+    GBK_CUDA(cudaMalloc(&f->col_new_to_old, 4 * nc1));
+    GBK_CUDA(cudaMalloc(&f->xr, eb * nc1));
+    GBK_CUDA(cudaMalloc(&cdeg, 4 * nc1));
+    GBK_CUDA(cudaMalloc(&cdeg_sorted, 4 * nc1));
+    GBK_CUDA(cudaMalloc(&iota, 4 * nc1));
+    GBK_CUDA(cudaMalloc(&old_to_new, 4 * nc1));
+    GBK_CUDA(cudaMalloc(&idx2, 4 * (nnz > 0 ? nnz : 1)));
+    GBK_CUDA(cudaMalloc(&acc, 8 * nc1));
+    GBK_CUDA(cudaMalloc(&thr, 8));
+    GBK_CUDA(cudaMemsetAsync(cdeg, 0, 4 * nc1, s));
+    GBK_CUDA(cudaMemsetAsync(thr, 0, 8, s));
+    const unsigned gs = (unsigned)std::min<int64_t>(blocks_for(nnz), 8 * num_sms());
+    if (nnz > 0) {
+        k_col_hist<<<blocks_for(nnz), 256, 0, s>>>(a.idx, nnz, cdeg);
+        GBK_LAUNCHED();
+    }
+    if (nc > 0) {
+        k_iota32<<<blocks_for(nc), 256, 0, s>>>(iota, nc);
+        GBK_LAUNCHED();
+        size_t tb = 0;
+        cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, cdeg, cdeg_sorted, iota, f->col_new_to_old, (int)nc, 0,
+                                                  32, s);
+        void* tmp = nullptr;
+        GBK_CUDA(cudaMalloc(&tmp, std::max<size_t>(tb, 16)));
+        GBK_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, tb, cdeg, cdeg_sorted, iota, f->col_new_to_old,
+                                                           (int)nc, 0, 32, s));
+        count_launch(1);
+        size_t sb = 0;
+        cub::DeviceScan::InclusiveSum(nullptr, sb, cdeg_sorted, acc, (int)nc, s);
+        void* stmp = nullptr;
+        GBK_CUDA(cudaMalloc(&stmp, std::max<size_t>(sb, 16)));
+        GBK_CUDA(cub::DeviceScan::InclusiveSum(stmp, sb, cdeg_sorted, acc, (int)nc, s));
+        count_launch(1);
+        k_dense_threshold<<<1, 1, 0, s>>>(acc, nc, (long long)(dense_frac * nnz), thr);
+        GBK_LAUNCHED();
+        k_invert_perm<<<blocks_for(nc), 256, 0, s>>>(f->col_new_to_old, nc, old_to_new);
+        GBK_LAUNCHED();
+        if (nnz > 0) {
+            k_relabel<<<gs, 256, 0, s>>>(a.idx, nnz, old_to_new, idx2);
+            GBK_LAUNCHED();
+        }
+        GBK_CUDA(cudaStreamSynchronize(s));
+        cudaFree(tmp);
+        cudaFree(stmp);
+    }
+    long long dense_cols = 0;
+    GBK_CUDA(cudaMemcpyAsync(&dense_cols, thr, 8, cudaMemcpyDeviceToHost, s));
+    GBK_CUDA(cudaStreamSynchronize(s));
+    f->dense_cols = dense_cols;
+    CsrView r = a;  // same rows and values, relabelled columns
+    r.idx = idx2;
+    r.bins = nullptr;
+    int rc = build_segsmem(r, dtype, &f->staged, s);
+    cudaFree(cdeg);
+    cudaFree(cdeg_sorted);
+    cudaFree(iota);
+    cudaFree(old_to_new);
+    cudaFree(idx2);
+    cudaFree(acc);
+    cudaFree(thr);
+    if (rc) {
+        free_seg(f);
+        return rc;
+    }
+    *out = f;
+    return GBK_SUCCESS;
+}
+
+// LAV (lav/build.hpp:97-212) without staging: columns renumbered by
+// in-degree, descending; the columns holding the first dense_frac of nnz form
+// "dense" segments of seg_cols columns, the rest one "sparse" segment; one
+// segment-major virtual CSR and an in-order merge.
 template <typename T>
 int build_lav(const CsrView& a, int32_t seg_cols, float dense_frac, SegCsr** out, cudaStream_t s) {
     std::vector<int64_t> cdeg;
@@ -1119,6 +1244,7 @@ int run_seg(const SegCsr* f, int accum, const T* x, T* y, cudaStream_t s) {
         GBK_LAUNCHED();
         xin = (const T*)f->xr;
     }
+    if (f->staged) return run_segsmem(f->staged, SR, accum, dtype_of_t<T>(), xin, y, s);
     if (f->nvrows > 0) {
         int rc = spmv_csr(f->v, SR, GBK_OP_SECOND, dtype_of_t<T>(), xin, f->partial, nullptr, 0, 0, s);
         if (rc) return rc;
@@ -1137,7 +1263,11 @@ int format_dispatch(gbk_matrix A, int orient, int sr, int accum, const T* x, T* 
     case SRV:                                                                  \
         if (A->format == GBK_FMT_SELL_C) return run_sell<SRV, T>(A->sell[orient], accum, x, y, s); \
         if (A->format == GBK_FMT_CSR_SEG) return run_seg<SRV, T>(A->seg[orient], accum, x, y, s);  \
-        return run_seg<SRV, T>(A->lav[orient], accum, x, y, s);
+        {                                                                      \
+            const int rc = run_seg<SRV, T>(A->lav[orient], accum, x, y, s);    \
+            if (rc != GBK_UNSUPPORTED) return rc;                              \
+        }                                                                      \
+        break;
     switch (sr) {
         FMT_CASE(GBK_PLUS_TIMES)
         FMT_CASE(GBK_LOR_LAND)
@@ -1226,6 +1356,8 @@ int build_format(gbk_matrix A, gbk_format fmt, const gbk_format_params* p, cudaS
         } else if (fmt == GBK_FMT_CSR_SEG) {
             rc = A->vtype == GBK_F32 ? build_seg<float>(v, prm.seg_cols, &A->seg[o], s)
                                      : build_seg<int32_t>(v, prm.seg_cols, &A->seg[o], s);
+        } else if (prm.seg_staged >= 0) {
+            rc = build_lav_staged(v, A->vtype, prm.lav_dense_frac, &A->lav[o], s);
         } else {
             rc = A->vtype == GBK_F32 ? build_lav<float>(v, prm.seg_cols, prm.lav_dense_frac, &A->lav[o], s)
                                      : build_lav<int32_t>(v, prm.seg_cols, prm.lav_dense_frac, &A->lav[o], s);
@@ -1247,7 +1379,8 @@ size_t format_bytes(gbk_matrix A) {
         }
         b += segsmem_bytes(A->segx[o]);
         const SegCsr* g = A->seg[o] ? A->seg[o] : A->lav[o];
-        if (g) b += g->v.nnz * (4 + eb) + (g->nvrows + 1) * 4 * 2 + (g->n + 1) * 4 + g->nvrows * eb;
+        if (g && g->staged) b += segsmem_bytes(g->staged) + g->ncols * (4 + eb);
+        else if (g) b += g->v.nnz * (4 + eb) + (g->nvrows + 1) * 4 * 2 + (g->n + 1) * 4 + g->nvrows * eb;
     }
     return b;
 }

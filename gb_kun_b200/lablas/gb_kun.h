@@ -15,3 +15,4 @@
 #include "lablas/matrix.hpp"
 #include "lablas/operations.hpp"
 #include "lablas/cblas_wrappers.hpp"
+#include "lablas/stats.hpp"

@@ -7,6 +7,7 @@
 #pragma once
 
 #include <algorithm>
+#include <memory>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -15,6 +16,36 @@
 #include "gbk_ingest.h"
 
 namespace lablas {
+
+template <typename T>
+class Matrix;
+
+namespace backend {
+
+// Host view of a matrix's CSR, the accessors of the reference's
+// backend::MatrixCSR (src/backend/matrix/csr/csr_matrix.h) that its
+// sequential checkers read (algorithms/*/ *_traditional.hpp reach it through
+// get_matrix()->get_csr()).  64-bit row pointers and column ids as there;
+// built from the matrix's host copy on first use.
+template <typename T>
+class MatrixCSR {
+public:
+    Index* get_row_ptr() { return row_ptr_.data(); }
+    const Index* get_row_ptr() const { return row_ptr_.data(); }
+    Index* get_col_ids() { return col_ids_.data(); }
+    const Index* get_col_ids() const { return col_ids_.data(); }
+    T* get_vals() { return vals_.get(); }
+    const T* get_vals() const { return vals_.get(); }
+    Index get_num_rows() const { return (Index)row_ptr_.size() - 1; }
+    Index get_nnz() const { return (Index)col_ids_.size(); }
+
+private:
+    friend class lablas::Matrix<T>;
+    std::vector<Index> row_ptr_, col_ids_;
+    std::unique_ptr<T[]> vals_;
+};
+
+}  // namespace backend
 
 template <typename T>
 class Matrix {
@@ -219,6 +250,19 @@ public:
     const std::vector<T>& host_val() const { return val_; }
     Matrix* get_matrix() { return this; }
     const Matrix* get_matrix() const { return this; }
+    // get_matrix()->get_csr() (src/backend/matrix/matrix.h): the host CSR view
+    const backend::MatrixCSR<T>* get_csr() const {
+        if (!csr_view_) {
+            auto* v = new backend::MatrixCSR<T>();
+            v->row_ptr_.assign(rp_.begin(), rp_.end());
+            if (v->row_ptr_.empty()) v->row_ptr_.push_back(0);
+            v->col_ids_.assign(col_.begin(), col_.end());
+            v->vals_.reset(new T[col_.size() > 0 ? col_.size() : 1]);
+            std::copy(val_.begin(), val_.end(), v->vals_.get());
+            csr_view_.reset(v);
+        }
+        return csr_view_.get();
+    }
 
     // Adopt a result computed on the device with the structure of `pattern`
     // (masked SpGEMM output, backend mxm).
@@ -296,6 +340,7 @@ private:
     void release() {
         if (h_) gbk_matrix_destroy(h_);
         h_ = nullptr;
+        csr_view_.reset();
     }
 
     gbk_matrix h_ = nullptr;
@@ -304,6 +349,7 @@ private:
     std::vector<int32_t> rp_, col_;
     std::vector<T> val_;
     std::vector<Index> rowdeg_, coldeg_;
+    mutable std::unique_ptr<backend::MatrixCSR<T>> csr_view_;
 };
 
 }  // namespace lablas

@@ -301,11 +301,56 @@ LA_Info extract(Vector<W>* w, const Vector<M>* mask, NULL_TYPE, const Vector<U>*
 // mxv / vxm (operations.h:152-211): dense input -> SpMV, sparse -> SpMSpV
 
 namespace detail {
+
+// dst = (D) src on the device, keeping src's current form (dense, or the
+// sparse id list with cast values).
+template <typename D, typename S>
+void cast_into(Vector<D>* dst, const Vector<S>* src) {
+    auto* s = const_cast<Vector<S>*>(src);
+    if (s->is_dense()) {
+        const S* sp = s->dense_ptr();
+        throw_if(gbk_vec_cast(sp, Vector<S>::dtype, dst->dense_ptr(), Vector<D>::dtype, s->size(), stream()),
+                 "cast");
+    } else {
+        const Index nv = s->sparse_nvals();
+        const int32_t* ids = s->ids_ptr();
+        const S* vals = s->vals_ptr();
+        dst->adopt_sparse(ids, nv, [&](D* out) {
+            throw_if(gbk_vec_cast(vals, Vector<S>::dtype, out, Vector<D>::dtype, nv, stream()), "cast");
+        });
+    }
+}
+
 template <typename W, typename M, typename A, typename U, typename BinaryOpTAccum, typename SemiringT>
-LA_Info mxv_impl(int transpose, Vector<W>* w, const Vector<M>* mask, BinaryOpTAccum, SemiringT,
+LA_Info mxv_same_type(int transpose, Vector<W>* w, const Vector<M>* mask, BinaryOpTAccum, SemiringT,
+                      const Matrix<A>* mat, const Vector<U>* u, Descriptor* desc);
+
+// mxv / vxm with element types that differ from the matrix's (the
+// reference's templates take W, M, a, U independently,
+// src/cpp_graphblas/operations.hpp:347-405): u and w are staged in the
+// matrix's element type on the device, the product runs there, and the
+// result is cast back into w.  Exact for the integer / boolean semirings;
+// a float semiring computes in the matrix's type.
+template <typename W, typename M, typename A, typename U, typename BinaryOpTAccum, typename SemiringT>
+LA_Info mxv_impl(int transpose, Vector<W>* w, const Vector<M>* mask, BinaryOpTAccum accum, SemiringT op,
                  const Matrix<A>* mat, const Vector<U>* u, Descriptor* desc) {
-    static_assert(std::is_same<W, A>::value && std::is_same<U, A>::value,
-                  "mxv / vxm run with matrix, input and output of one element type");
+    if constexpr (std::is_same<W, A>::value && std::is_same<U, A>::value) {
+        return mxv_same_type(transpose, w, mask, accum, op, mat, u, desc);
+    } else {
+        Vector<A> ua(u->size());
+        Vector<A> wa(w->size());
+        cast_into(&ua, u);
+        cast_into(&wa, w);
+        LA_Info rc = mxv_same_type(transpose, &wa, mask, accum, op, mat, &ua, desc);
+        if (rc != GrB_SUCCESS) return rc;
+        cast_into(w, &wa);
+        return GrB_SUCCESS;
+    }
+}
+
+template <typename W, typename M, typename A, typename U, typename BinaryOpTAccum, typename SemiringT>
+LA_Info mxv_same_type(int transpose, Vector<W>* w, const Vector<M>* mask, BinaryOpTAccum, SemiringT,
+                      const Matrix<A>* mat, const Vector<U>* u, Descriptor* desc) {
     const gbk_semiring sr = SemiringT::gbk_sr;
     const gbk_binop acc = accum_code<BinaryOpTAccum>();
     const Desc_value mode = mask_mode(desc);
@@ -406,22 +451,33 @@ LA_Info mxm(Matrix<c>* C, const Matrix<m>* mask, NULL_TYPE, SemiringT op, const 
 
 /* Matrix: same structure as u, values op(u_ij, i, j, val) (select.h:363-395,
  * which accumulates into 0, so the accumulator and the mask do not act). */
+namespace detail {
+// A generic C++ callable (a lambda, as in the reference's
+// algorithms/tc/tc.hpp:55-70) is host code and cannot run on the device;
+// there is no host fallback, so such a select throws when it is called.
+[[noreturn]] inline void select_needs_tagged_operator() {
+    throw "Error: select with a generic callable cannot run on the device; use lablas::TrilSelect, TriuSelect, "
+          "DiagSelect, OffdiagSelect or ValueEq/Ne/Gt/Ge/Lt/LeSelect";
+}
+}  // namespace detail
+
 template <typename W, typename M, typename U, typename T, typename BinaryOpT, typename SelectOpT>
 LA_Info select(Matrix<W>* w, const Matrix<M>* mask, BinaryOpT accum, SelectOpT op, const Matrix<U>* u, const T val,
                Descriptor* desc) {
-    static_assert(is_select_op<SelectOpT>::value,
-                  "select on the device takes a tagged operator: lablas::TrilSelect, TriuSelect, DiagSelect, "
-                  "OffdiagSelect, ValueEq/Ne/Gt/Ge/Lt/LeSelect");
     static_assert(std::is_same<W, U>::value, "select keeps the value type of u");
     (void)mask;
     (void)accum;
     (void)op;
     (void)desc;
     if (detail::null_any(w, u)) return GrB_UNINITIALIZED_OBJECT;
-    gbk_matrix out = nullptr;
-    int rc = gbk_select_matrix(&out, u->handle(), SelectOpT::gbk_sel, (double)val, stream());
-    if (rc) return detail::done(rc);
-    return w->adopt_handle(out);
+    if constexpr (!is_select_op<SelectOpT>::value) {
+        detail::select_needs_tagged_operator();
+    } else {
+        gbk_matrix out = nullptr;
+        int rc = gbk_select_matrix(&out, u->handle(), SelectOpT::gbk_sel, (double)val, stream());
+        if (rc) return detail::done(rc);
+        return w->adopt_handle(out);
+    }
 }
 template <typename W, typename M, typename U, typename T, typename SelectOpT>
 LA_Info select(Matrix<W>* w, const Matrix<M>* mask, NULL_TYPE, SelectOpT op, const Matrix<U>* u, const T val,
@@ -429,17 +485,10 @@ LA_Info select(Matrix<W>* w, const Matrix<M>* mask, NULL_TYPE, SelectOpT op, con
     return select(w, mask, second<W, U, W>(), op, u, val, desc);
 }
 
-/* Vector: w[i] = accum(w[i], op(u[i], i, 0, val)) where the mask selects;
- * GrB_REPLACE zeroes the rest (select.h:17-315). */
-template <typename W, typename M, typename U, typename T, typename BinaryOpT, typename SelectOpT>
-LA_Info select(Vector<W>* w, const Vector<M>* mask, BinaryOpT accum, SelectOpT op, const Vector<U>* u, const T val,
-               Descriptor* desc) {
-    static_assert(is_select_op<SelectOpT>::value,
-                  "select on the device takes a tagged operator: lablas::TrilSelect, TriuSelect, DiagSelect, "
-                  "OffdiagSelect, ValueEq/Ne/Gt/Ge/Lt/LeSelect");
-    (void)accum;
-    (void)op;
-    if (detail::null_any(w, u)) return GrB_UNINITIALIZED_OBJECT;
+namespace detail {
+template <typename SelectOpT, typename W, typename M, typename U, typename T, typename BinaryOpT>
+LA_Info select_vector_tagged(Vector<W>* w, const Vector<M>* mask, BinaryOpT, const Vector<U>* u, const T val,
+                             Descriptor* desc) {
     if (w->size() != u->size()) return GrB_DIMENSION_MISMATCH;
     if (mask && mask->size() != w->size()) return GrB_DIMENSION_MISMATCH;
     const U* up = u->dense_ptr();
@@ -452,6 +501,23 @@ LA_Info select(Vector<W>* w, const Vector<M>* mask, BinaryOpT accum, SelectOpT o
                                           Vector<U>::dtype, w->size(), BinaryOpT::gbk_code, mask ? &m : nullptr,
                                           mask && out_mode == GrB_REPLACE, stream()));
 }
+}  // namespace detail
+
+/* Vector: w[i] = accum(w[i], op(u[i], i, 0, val)) where the mask selects;
+ * GrB_REPLACE zeroes the rest (select.h:17-315). */
+template <typename W, typename M, typename U, typename T, typename BinaryOpT, typename SelectOpT>
+LA_Info select(Vector<W>* w, const Vector<M>* mask, BinaryOpT accum, SelectOpT op, const Vector<U>* u, const T val,
+               Descriptor* desc) {
+    (void)accum;
+    (void)op;
+    if (detail::null_any(w, u)) return GrB_UNINITIALIZED_OBJECT;
+    if constexpr (!is_select_op<SelectOpT>::value) {
+        detail::select_needs_tagged_operator();
+    } else {
+        return detail::select_vector_tagged<SelectOpT>(w, mask, accum, u, val, desc);
+    }
+}
+
 template <typename W, typename M, typename U, typename T, typename SelectOpT>
 LA_Info select(Vector<W>* w, const Vector<M>* mask, NULL_TYPE, SelectOpT op, const Vector<U>* u, const T val,
                Descriptor* desc) {

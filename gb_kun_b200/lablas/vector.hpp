@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <iostream>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -18,23 +19,38 @@ namespace lablas {
 template <typename T>
 class Vector;
 
-// Host view returned by get_vector()->getDense() (read-only copy).
+// Host view returned by get_vector()->getDense(): a host copy of the dense
+// form.  Through the non-const getDense() the caller may also write it (the
+// reference's sequential checkers fill their result vectors this way); the
+// vector then treats the host copy as the newer one and uploads it before
+// its next device operation.  Plain array storage, so Vector<bool> has a
+// bool* like every other element type.
 template <typename T>
 class HostDenseView {
 public:
-    const T* get_vals() const { return vals_.data(); }
-    T* get_vals() { return vals_.data(); }
-    Index get_size() const { return (Index)vals_.size(); }
+    const T* get_vals() const { return vals_.get(); }
+    T* get_vals() { return vals_.get(); }
+    Index get_size() const { return n_; }
     Index get_nvals() const {
         Index c = 0;
-        for (auto& v : vals_) c += (v != T(0));
+        for (Index i = 0; i < n_; i++) c += (vals_[i] != T(0));
         return c;
     }
 
 private:
     template <typename U>
     friend class Vector;
-    std::vector<T> vals_;
+    void resize(Index n) {
+        if (n == n_ && vals_) return;
+        vals_.reset(new T[n > 0 ? n : 1]);
+        n_ = n;
+    }
+    void swap(HostDenseView& o) {
+        std::swap(vals_, o.vals_);
+        std::swap(n_, o.n_);
+    }
+    std::unique_ptr<T[]> vals_;
+    Index n_ = 0;
 };
 
 template <typename T>
@@ -65,8 +81,8 @@ public:
         if (values == nullptr) return GrB_NULL_POINTER;
         if (nvals == 0) return GrB_INVALID_VALUE;
         ensure_dense_buf();
-        std::vector<T> tmp(values, values + std::min<Index>(nvals, n_));
-        dense_.upload(tmp.data(), tmp.size());
+        const Index m = std::min<Index>(nvals, n_);
+        if (m > 0) dense_.upload(values, m);
         dense_mode_ = true;
         return GrB_SUCCESS;
     }
@@ -123,6 +139,7 @@ public:
         return GrB_SUCCESS;
     }
     Index nvals() const {
+        sync_host();
         if (!dense_mode_) return nvals_;
         if (n_ == 0) return 0;
         int64_t c = 0;
@@ -136,7 +153,8 @@ public:
         std::swap(dense_mode_, o->dense_mode_);
         std::swap(nvals_, o->nvals_);
         std::swap(host_valid_, o->host_valid_);
-        std::swap(view_.vals_, o->view_.vals_);
+        std::swap(host_newer_, o->host_newer_);
+        view_.swap(o->view_);
         dense_.swap(o->dense_);
         ids_.swap(o->ids_);
         vals_.swap(o->vals_);
@@ -151,6 +169,7 @@ public:
     }
     LA_Info dup(const Vector<T>* rhs) {
         touch();
+        rhs->sync_host();
         if (rhs->n_ != n_) return GrB_DIMENSION_MISMATCH;
         dense_mode_ = rhs->dense_mode_;
         if (dense_mode_) {
@@ -180,14 +199,21 @@ public:
     }
     void print_storage_type() const { std::cout << (dense_mode_ ? "dense" : "sparse") << std::endl; }
 
-    // ---- backend-style access (reference drivers read host arrays this way) ----
+    // ---- backend-style access (reference drivers and checkers read and write
+    // host arrays this way) ----
     Vector* get_vector() { return this; }
     const Vector* get_vector() const { return this; }
+    // Writable host copy: the caller may change it, so it becomes the newer
+    // copy and is uploaded before the next device operation on this vector.
     HostDenseView<T>* getDense() {
         host_dense();
+        host_newer_ = true;
         return &view_;
     }
-    const HostDenseView<T>* getDense() const { return const_cast<Vector*>(this)->getDense(); }
+    const HostDenseView<T>* getDense() const {
+        const_cast<Vector*>(this)->host_dense();
+        return &view_;
+    }
 
     // ---- device form, used by the operations ----
     bool is_dense() const { return dense_mode_; }
@@ -195,6 +221,7 @@ public:
     Storage get_storage() const { return dense_mode_ ? GrB_DENSE : GrB_SPARSE; }
 
     void force_to_dense() {
+        sync_host();
         ensure_dense_buf();
         if (dense_mode_) return;
         ensure_sparse_buf();
@@ -202,6 +229,7 @@ public:
         dense_mode_ = true;
     }
     void force_to_sparse() {
+        sync_host();
         ensure_sparse_buf();
         if (!dense_mode_) return;
         ensure_dense_buf();
@@ -240,6 +268,7 @@ public:
     }
     // mask argument in its current form
     gbk_mask as_mask(Desc_value mode) const {
+        sync_host();
         gbk_mask m{};
         m.mode = (int32_t)mode;
         if (dense_mode_) {
@@ -254,16 +283,44 @@ public:
     }
     // host copy of the dense form (forces the dense form, as getDense() does)
     const T* host_dense() {
+        if (host_newer_) return view_.get_vals();
         force_to_dense();
         if (!host_valid_) {
-            view_.vals_.resize(n_);
-            if (n_) dense_.download(view_.vals_.data(), n_);
+            view_.resize(n_);
+            if (n_) dense_.download(view_.vals_.get(), n_);
             host_valid_ = true;
         }
-        return view_.vals_.data();
+        return view_.get_vals();
+    }
+    // Sparse form with the ids of another device list (copied) and values
+    // written by fill_vals into this vector's value buffer.
+    template <typename F>
+    void adopt_sparse(const int32_t* ids, Index nv, F&& fill_vals) {
+        touch();
+        ensure_sparse_buf();
+        if (nv) {
+            cuda_check(cudaMemcpyAsync(ids_.p, ids, sizeof(int32_t) * nv, cudaMemcpyDeviceToDevice,
+                                       current_stream()), "adopt_sparse");
+            fill_vals(vals_.p);
+        }
+        nvals_ = nv;
+        dense_mode_ = false;
+    }
+    // A host copy handed out writable goes back to the device first.
+    void sync_host() const {
+        auto* self = const_cast<Vector*>(this);
+        if (!self->host_newer_) return;
+        self->host_newer_ = false;
+        self->ensure_dense_buf();
+        if (n_) self->dense_.upload(self->view_.vals_.get(), n_);
+        self->dense_mode_ = true;
+        self->host_valid_ = true;
     }
     // every device-side change drops the host copy
-    void touch() { host_valid_ = false; }
+    void touch() {
+        sync_host();
+        host_valid_ = false;
+    }
 
 private:
     LA_Info build_sparse(const Index* ids, const T* vals, Index nvals) {
@@ -297,6 +354,7 @@ private:
     DeviceBuffer<T> vals_;
     HostDenseView<T> view_;
     bool host_valid_ = false;
+    bool host_newer_ = false;
     std::string name_;
 
     template <typename Y>

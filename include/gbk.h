@@ -149,6 +149,18 @@ int gbk_mxv_sparse_mask(gbk_matrix A, int transpose, gbk_semiring sr, gbk_binop 
 int gbk_spmspv(gbk_matrix A, int transpose, gbk_semiring sr, gbk_binop accum, gbk_dtype dtype,
                const int32_t* x_ids, const void* x_vals, int64_t x_nvals, void* y, const gbk_mask* mask,
                void* stream);
+/* Push SpMSpV with a sparse output (spmspv_unmasked_or_map /
+ * spmspv_unmasked_critical_map, src/backend/spmspv/spmspv_maps.h:5-142, the
+ * SparseVector form of backend::SpMSpV, spmspv.h:162-205): every row reached
+ * from the frontier appears once in (y_ids, y_vals), ids ascending, its value
+ * the semiring's add over its products; when add probes to 1 (or-monoids)
+ * every reached row holds 1.  y_ids / y_vals need room for the number of rows
+ * of the output (at most the distinct reached rows are written); *y_nvals is
+ * written on the host (the call synchronises the stream).  A mask is refused
+ * (GBK_UNSUPPORTED) as the reference throws for it. */
+int gbk_spmspv_sparse(gbk_matrix A, int transpose, gbk_semiring sr, gbk_dtype dtype, const int32_t* x_ids,
+                      const void* x_vals, int64_t x_nvals, int32_t* y_ids, void* y_vals, int64_t* y_nvals,
+                      const gbk_mask* mask, void* stream);
 
 /* ---- SpGEMM ------------------------------------------------------------- */
 

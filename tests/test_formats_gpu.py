@@ -131,12 +131,14 @@ def test_masked_call_uses_csr_semantics(capi, oracle):
     assert np.array_equal(y.cpu().numpy(), oracle.mxv("lor_land", g, val, x, y0, mask=m, mask_mode=5))
 
 
+@pytest.mark.parametrize("fmt", ["CSR_SEG", "LAV"])
 @pytest.mark.parametrize("sr", ["plus_times", "min_plus", "lor_land", "plus_one", "min_second", "first_wins"])
 @pytest.mark.parametrize("accum", ["second", "plus"])
-def test_staged_segments_many_windows(capi, oracle, sr, accum):
-    """CSR_SEG with x windows in shared memory on a graph of 3 windows (131072
-    columns), every add class (atomic add / min / or) and the CSR fallback
-    for a non-associative add; float sums within REL_L1_TOL, integers exact."""
+def test_staged_segments_many_windows(capi, oracle, fmt, sr, accum):
+    """CSR_SEG, and LAV (columns renumbered by in-degree on the device), with
+    x windows in shared memory on a graph of 3 windows (131072 columns),
+    every add class (atomic add / min / or) and the CSR fallback for a
+    non-associative add; float sums within REL_L1_TOL, integers exact."""
     g = gg.rmat(17, 12, seed=8)
     if sr == "plus_times":
         val = gg.values_f32(g, seed=1)
@@ -148,7 +150,7 @@ def test_staged_segments_many_windows(capi, oracle, sr, accum):
         x[::5] = 0
         y0 = np.full(g.n, 7, np.int32)
     A = capi.Matrix.from_graph(g, val)
-    A.set_format("CSR_SEG")
+    A.set_format(fmt)
     for transpose in (False, True):
         y = dev(y0.copy())
         A.mxv(dev(x), y, semiring=sr, accum=accum, transpose=transpose)
@@ -160,3 +162,23 @@ def test_staged_segments_many_windows(capi, oracle, sr, accum):
             assert rel_l1(got, expect) < REL_L1_TOL, (transpose, rel_l1(got, expect))
         else:
             assert np.array_equal(got, expect), (sr, accum, transpose)
+
+
+def test_lav_renumbering_matches_reference_order(capi, oracle):
+    """The device LAV build orders columns by in-degree, descending, ties in
+    column order (lav/build.hpp:113-141): the result must not depend on it,
+    but the staged and the unstaged LAV (both renumbered) must agree exactly
+    on an integer semiring, and both with the oracle."""
+    g = gg.rmat(16, 16, seed=9)
+    val = gg.weights_i32(g, seed=3, lo=1, hi=100)
+    x = (gg.vector_f32(g.n, seed=4) * 1000).astype(np.int32)
+    y0 = np.zeros(g.n, np.int32)
+    want = oracle.mxv("min_plus", g, val, x, y0)
+    A = capi.Matrix.from_graph(g, val)
+    outs = []
+    for staged in (0, -1):
+        A.set_format("LAV", seg_staged=staged)
+        y = dev(y0.copy())
+        A.mxv(dev(x), y, semiring="min_plus")
+        outs.append(y.cpu().numpy())
+    assert np.array_equal(outs[0], want) and np.array_equal(outs[1], want)

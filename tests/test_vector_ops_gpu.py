@@ -246,3 +246,57 @@ def test_mxm_masked_counts(capi, oracle):
     capi.check(capi.lib().gbk_reduce(0, capi.I64, ctypes.c_void_p(v), capi.I32, g.nnz, ctypes.byref(out),
                                      capi.stream_ptr()), "gbk_reduce")
     assert out.value == 6 * oracle.tc(g)
+
+
+@pytest.mark.parametrize("sr,dtype", [("lor_land", "f32"), ("plus_times", "f32"), ("min_plus", "i32"),
+                                      ("min_second", "i32"), ("plus_one", "i32"), ("custom_less_plus", "f32")])
+@pytest.mark.parametrize("transpose", [False, True])
+@pytest.mark.parametrize("nf", [0, 1, 150, 2048])
+def test_spmspv_sparse_output_vs_oracle(capi, oracle, sr, dtype, transpose, nf):
+    """The map-based sparse-output push (spmspv_maps.h:5-142): every reached row
+    once, ids ascending, value = the semiring's add over its products (or 1
+    when add probes to 1, as the or-map and a less-monoid do)."""
+    g = gg.rmat(11, 16, seed=23)
+    val = gg.values_f32(g, seed=1) if dtype == "f32" else gg.weights_i32(g, seed=1, lo=1, hi=50)
+    A = capi.Matrix.from_graph(g, val)
+    r = rng(11)
+    f_ids = np.sort(r.choice(g.n, nf, replace=False)).astype(np.int32)
+    f_vals = (r.random(nf) * 10 + 1).astype(val.dtype)
+    ids, vals = A.spmspv_sparse(dev(f_ids), dev(f_vals), semiring=sr, transpose=transpose)
+    if transpose:
+        go, vo = g, val
+    else:
+        cp, row, _ = oracle.transpose(g)
+        rows = np.repeat(np.arange(g.n), g.degrees())
+        vo = val[np.lexsort((rows, g.col))]
+        go = gg.Graph(n=g.n, row_ptr=cp, col=row)
+    reached = np.unique(np.concatenate([go.col[go.row_ptr[i]:go.row_ptr[i + 1]] for i in f_ids])
+                        if nf else np.zeros(0, np.int32))
+    assert np.array_equal(ids.cpu().numpy(), reached.astype(np.int32))
+    got = vals.cpu().numpy()
+    if sr in ("lor_land", "custom_less_plus"):
+        assert (got == 1).all()
+        return
+    ident = {"plus_times": 0, "plus_one": 0, "min_plus": np.iinfo(np.int32).max,
+             "min_second": np.iinfo(np.int32).max}[sr]
+    y0 = np.full(g.n, ident, val.dtype)
+    dense = oracle.spmspv(sr, go, vo, f_ids, f_vals, y0)
+    if sr == "plus_times":
+        assert rel_l1(got, dense[reached]) < REL_L1_TOL
+    else:
+        assert np.array_equal(got, dense[reached])
+
+
+def test_spmspv_sparse_output_refuses_a_mask(capi):
+    g = gg.rmat(8, 8, seed=24)
+    A = capi.Matrix.from_graph(g, gg.values_f32(g))
+    ids = dev(np.array([1, 2], np.int32))
+    vals = dev(np.ones(2, np.float32))
+    m = capi.dense_mask(dev(np.ones(g.n, np.float32)))
+    import ctypes as C
+    y_ids = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    y_vals = torch.empty(g.n, dtype=torch.float32, device="cuda")
+    nv = C.c_int64()
+    rc = capi.lib().gbk_spmspv_sparse(A.h, 0, capi.SEMIRING["plus_times"], capi.F32, capi.ptr(ids), capi.ptr(vals), 2,
+                                      capi.ptr(y_ids), capi.ptr(y_vals), C.byref(nv), C.byref(m), capi.stream_ptr())
+    assert rc == 21  # GBK_UNSUPPORTED
