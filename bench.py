@@ -62,6 +62,9 @@ def parse():
     p.add_argument("--format", default="auto", choices=["auto", "CSR", "SELL_C", "CSR_SEG", "LAV"],
                    help="storage format; auto = the per-graph autotuner's choice")
     p.add_argument("--sigma", type=int, default=0, help="SELL-C sorting window for --format SELL_C")
+    p.add_argument("--staged", type=int, default=0,
+                   help="--format SELL_C: 1 = SELL-C-sigma inside staged x windows; CSR_SEG / LAV: -1 = unstaged")
+    p.add_argument("--reorder", type=int, default=0, help="--format SELL_C: renumber columns by in-degree")
     p.add_argument("--seed", type=int, default=42)
     p.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -250,9 +253,12 @@ def read_traffic(profile):
     return found.get("traffic_bytes_per_spmv:", found.get("traffic_bytes_per_launch:"))
 
 
-def dominant_kernel(fmt_name, scale, graph):
+def dominant_kernel(fmt_name, scale, graph, staged=False):
     """(kernel description, profile summary) for the storage format that ran."""
     tag = f"{graph}{scale}"
+    if fmt_name == "SELL_C" and staged:
+        return ("k_sellw (SELL-C-sigma inside x windows staged in shared memory; + k_sw_prologue for y and the "
+                "renumbered x); achieved counts the whole SpMV", f"spmv_sell_c_staged_{tag}")
     if fmt_name == "SELL_C":
         return ("k_sell_items (+ k_piece_fold for long-row pieces, k_sell_fold, k_spmv_binned for the few "
                 "problematic slices); achieved counts the whole SpMV", f"spmv_sell_c_{tag}")
@@ -295,7 +301,9 @@ def format_sweep(args, peak):
             ("SELL_C_s4096", {"fmt": "SELL_C", "sigma": 4096}),
             ("SELL_C_s4096_reorder", {"fmt": "SELL_C", "sigma": 4096, "reorder": 1}),
             ("SELL_C_s256_reorder", {"fmt": "SELL_C", "sigma": 256, "reorder": 1}),
-            ("CSR_SEG", {"fmt": "CSR_SEG"}), ("LAV", {"fmt": "LAV"})]
+            ("CSR_SEG", {"fmt": "CSR_SEG"}), ("LAV", {"fmt": "LAV"}),
+            ("SELL_C_staged", {"fmt": "SELL_C", "staged": 1}),
+            ("SELL_C_staged_reorder", {"fmt": "SELL_C", "staged": 1, "reorder": 1})]
     for gname in ("rmat", "er"):
         g = gg.rmat(args.scale, args.edge_factor, seed=args.seed) if gname == "rmat" else \
             gg.uniform(args.scale, args.edge_factor, seed=args.seed)
@@ -308,7 +316,7 @@ def format_sweep(args, peak):
         dy = torch.zeros(g.n, device="cuda")
         for name, f in fmts:
             A.set_format(f["fmt"], sigma=f.get("sigma", 0), csr_kernel=f.get("csr_kernel", 0), hot_cols=f.get("hot", 0),
-                         reorder_cols=f.get("reorder", 0))
+                         reorder_cols=f.get("reorder", 0), seg_staged=f.get("staged", 0))
             ms = time_spmv(A, dx, dy, args.sweep_steps, 3)
             err = float(np.abs(dy.cpu().numpy().astype(np.float64) - ref).sum() / np.abs(ref).sum())
             ms_or = time_spmv(A, dx, dy, args.sweep_steps, 3, semiring="lor_land")
@@ -462,7 +470,7 @@ def run_ours(args):
         if args.format == "auto":
             tuned = A.autotune(reps=20).describe()
         else:
-            A.set_format(args.format, sigma=args.sigma)
+            A.set_format(args.format, sigma=args.sigma, seg_staged=args.staged, reorder_cols=args.reorder)
         for _ in range(args.warmup):
             A.mxv(dx, dy)
         torch.cuda.synchronize()
@@ -500,7 +508,8 @@ def run_ours(args):
 
     peak, peak_kind = hbm_peak()
     ran_format = tuned["format"] if tuned else args.format
-    kern_desc, kern_profile = dominant_kernel(ran_format, args.scale, args.graph)
+    staged = bool(tuned.get("staged_windows")) if tuned else args.staged == 1
+    kern_desc, kern_profile = dominant_kernel(ran_format, args.scale, args.graph, staged)
     # one launch = one SpMV (the y initialisation and the main kernel, which
     # starts under programmatic dependent launch); its average duration is
     # the per-step time of the timed region
@@ -513,7 +522,8 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded R-MAT, generated in-process)",
         "config": cfg,
-        "format_ran": tuned if tuned else {"format": args.format, "sigma": args.sigma},
+        "format_ran": tuned if tuned else {"format": args.format, "sigma": args.sigma, "staged": args.staged,
+                                           "reorder_cols": args.reorder},
         "pct_hbm_peak": round(100 * achieved / peak, 2),
         "gteps": round(world * g.nnz / (ms_per_step * 1e-3) / 1e9, 3),
         "ref_formula_gbs": round(world * 16 * g.nnz / (ms_per_step * 1e-3) / 1e9, 2),

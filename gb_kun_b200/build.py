@@ -35,6 +35,7 @@ CU_SOURCES = [
     "spmv_bins.cu",
     "spmv_formats.cu",
     "spmv_segsmem.cu",
+    "spmv_sellw.cu",
     "spmspv.cu",
     "spmspv_sparse.cu",
     "vector_ops.cu",

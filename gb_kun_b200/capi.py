@@ -62,12 +62,12 @@ class MatrixInfo(C.Structure):
 
 class TuneResult(C.Structure):
     _fields_ = [("format", C.c_int32), ("sell_sigma", C.c_int32), ("csr_kernel", C.c_int32), ("cached", C.c_int32),
-                ("ncandidates", C.c_int32), ("best_ms", C.c_float), ("candidate_ms", C.c_float * 12),
-                ("sell_hot_cols", C.c_int32)]
+                ("ncandidates", C.c_int32), ("best_ms", C.c_float), ("candidate_ms", C.c_float * 16),
+                ("sell_hot_cols", C.c_int32), ("sell_staged", C.c_int32)]
 
     CANDIDATES = ["CSR_bins", "CSR_merge", "SELL_C_s1", "SELL_C_s256", "SELL_C_s4096", "CSR_SEG", "LAV",
                   "SELL_C_s4096_hot16k", "SELL_C_s4096_hot52k", "SELL_C_s256_hot52k", "SELL_C_s4096_reorder",
-                  "SELL_C_s256_reorder"]
+                  "SELL_C_s256_reorder", "SELL_C_staged", "SELL_C_staged_reorder"]
 
     def describe(self) -> dict:
         names = {0: "CSR", 3: "CSR_SEG", 4: "LAV", 6: "SELL_C"}
@@ -75,6 +75,7 @@ class TuneResult(C.Structure):
         if self.format == 6:
             d["sigma"] = self.sell_sigma
             d["hot_cols"] = self.sell_hot_cols
+            d["staged_windows"] = bool(self.sell_staged)
         if self.format == 0:
             d["csr_kernel"] = {1: "merge-path", 2: "degree-bins"}.get(self.csr_kernel, "default")
         if not self.cached:

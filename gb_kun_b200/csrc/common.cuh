@@ -188,6 +188,27 @@ template <typename T> struct Semiring<GBK_PLUS_ONE, T> {
 // otherwise a generic read-modify-write.
 int semiring_probe(int sr, int dtype);
 
+// Atomic folds of a semiring sum into y (the staged-window kernels).
+__device__ __forceinline__ void atomic_min_any(float* p, float v) {
+    // order-preserving on the bit patterns: non-negative floats order as ints,
+    // negative ones in reverse as unsigned ints
+    if (v >= 0.0f)
+        atomicMin((int*)p, __float_as_int(v));
+    else
+        atomicMax((unsigned int*)p, __float_as_uint(v));
+}
+__device__ __forceinline__ void atomic_min_any(int32_t* p, int32_t v) { atomicMin(p, v); }
+
+__device__ __forceinline__ void atomic_add_any(float* p, float v) { atomicAdd(p, v); }
+__device__ __forceinline__ void atomic_add_any(int32_t* p, int32_t v) {
+    // saturating, like elem_add, so INT_MAX stays the min-plus infinity
+    int old = *((volatile int*)p), assumed;
+    do {
+        assumed = old;
+        old = atomicCAS(p, assumed, elem_add(assumed, v));
+    } while (old != assumed);
+}
+
 // ----------------------------------------------------------------------------
 // binary operators (accumulators), runtime-selected: applied once per output.
 

@@ -39,6 +39,7 @@ struct CsrView {
 struct SellC;     // spmv_formats.cu
 struct SegCsr;    // spmv_formats.cu (CSR_SEG and LAV share one layout)
 struct SegSmem;   // spmv_segsmem.cu (CSR_SEG with x windows staged in shared memory)
+struct SellW;     // spmv_sellw.cu (SELL-C-sigma inside x windows staged in shared memory)
 struct Batch;     // batched.h
 
 // Tunables of the batched traversals (batched.cu).
@@ -66,6 +67,7 @@ struct gbk_matrix_s {
     gbk::SegCsr* seg[2] = {nullptr, nullptr};
     gbk::SegCsr* lav[2] = {nullptr, nullptr};
     gbk::SegSmem* segx[2] = {nullptr, nullptr};
+    gbk::SellW* sellw[2] = {nullptr, nullptr};
     void* xcopy = nullptr;      // n elements, used when x aliases y
     int64_t xcopy_elems = 0;
     int device = 0;
@@ -108,5 +110,16 @@ int run_segsmem(const SegSmem* f, int sr, int accum, int dtype, const void* x, v
 void free_segsmem(SegSmem* f);
 size_t segsmem_bytes(const SegSmem* f);
 int64_t format_padded_nnz(gbk_matrix A);
+// SELL-C-sigma inside staged x windows (spmv_sellw.cu); run_sellw returns
+// GBK_UNSUPPORTED for semirings whose add it cannot fold atomically.
+int build_sellw(const CsrView& a, int dtype, bool reorder, SellW** out, cudaStream_t s);
+int run_sellw(const SellW* f, int sr, int accum, int dtype, const void* x, void* y, cudaStream_t s);
+void free_sellw(SellW* f);
+size_t sellw_bytes(const SellW* f);
+int64_t sellw_padded(const SellW* f);
+// Column order by in-degree (spmv_formats.cu): new_to_old and relabelled
+// column ids, both cudaMalloc'd for the caller.
+int indegree_order(const CsrView& a, float dense_frac, int32_t** new_to_old, int32_t** idx_out,
+                   int64_t* dense_cols, cudaStream_t s);
 
 }  // namespace gbk

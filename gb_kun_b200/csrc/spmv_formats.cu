@@ -1066,17 +1066,22 @@ int build_seg(const CsrView& a, int32_t seg_cols, SegCsr** out, cudaStream_t s) 
 // the reference's one "sparse" segment becomes the remaining windows, staged
 // the same way.  x is gathered into the new order on every call
 // (spmv_lav.h:24-26).
-int build_lav_staged(const CsrView& a, int dtype, float dense_frac, SegCsr** out, cudaStream_t s) {
+}  // namespace
+
+// Column order by in-degree, descending, ties in column order (the
+// reference's LAV order, lav/build.hpp:113-141), computed on the device:
+// *new_to_old (ncols) and the column ids relabelled into *idx_out (nnz), both
+// allocated here (cudaMalloc, the caller frees them); *dense_cols = the
+// first renumbered column at which the running in-degree sum reaches
+// dense_frac of nnz.
+int indegree_order(const CsrView& a, float dense_frac, int32_t** new_to_old, int32_t** idx_out,
+                   int64_t* dense_cols, cudaStream_t s) {
     const int64_t nc = a.ncols, nnz = a.nnz;
-    SegCsr* f = new SegCsr();
-    f->n = a.nrows;
-    f->ncols = nc;
-    const size_t eb = dtype == GBK_F32 ? sizeof(float) : sizeof(int32_t);
-    int32_t *cdeg = nullptr, *cdeg_sorted = nullptr, *iota = nullptr, *old_to_new = nullptr, *idx2 = nullptr;
+    int32_t *cdeg = nullptr, *cdeg_sorted = nullptr, *iota = nullptr, *old_to_new = nullptr, *idx2 = nullptr,
+            *n2o = nullptr;
     long long *acc = nullptr, *thr = nullptr;
     const int64_t nc1 = nc > 0 ? nc : 1;
-    GBK_CUDA(cudaMalloc(&f->col_new_to_old, 4 * nc1));
-    GBK_CUDA(cudaMalloc(&f->xr, eb * nc1));
+    GBK_CUDA(cudaMalloc(&n2o, 4 * nc1));
     GBK_CUDA(cudaMalloc(&cdeg, 4 * nc1));
     GBK_CUDA(cudaMalloc(&cdeg_sorted, 4 * nc1));
     GBK_CUDA(cudaMalloc(&iota, 4 * nc1));
@@ -1095,12 +1100,10 @@ int build_lav_staged(const CsrView& a, int dtype, float dense_frac, SegCsr** out
         k_iota32<<<blocks_for(nc), 256, 0, s>>>(iota, nc);
         GBK_LAUNCHED();
         size_t tb = 0;
-        cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, cdeg, cdeg_sorted, iota, f->col_new_to_old, (int)nc, 0,
-                                                  32, s);
+        cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, cdeg, cdeg_sorted, iota, n2o, (int)nc, 0, 32, s);
         void* tmp = nullptr;
         GBK_CUDA(cudaMalloc(&tmp, std::max<size_t>(tb, 16)));
-        GBK_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, tb, cdeg, cdeg_sorted, iota, f->col_new_to_old,
-                                                           (int)nc, 0, 32, s));
+        GBK_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, tb, cdeg, cdeg_sorted, iota, n2o, (int)nc, 0, 32, s));
         count_launch(1);
         size_t sb = 0;
         cub::DeviceScan::InclusiveSum(nullptr, sb, cdeg_sorted, acc, (int)nc, s);
@@ -1110,7 +1113,7 @@ int build_lav_staged(const CsrView& a, int dtype, float dense_frac, SegCsr** out
         count_launch(1);
         k_dense_threshold<<<1, 1, 0, s>>>(acc, nc, (long long)(dense_frac * nnz), thr);
         GBK_LAUNCHED();
-        k_invert_perm<<<blocks_for(nc), 256, 0, s>>>(f->col_new_to_old, nc, old_to_new);
+        k_invert_perm<<<blocks_for(nc), 256, 0, s>>>(n2o, nc, old_to_new);
         GBK_LAUNCHED();
         if (nnz > 0) {
             k_relabel<<<gs, 256, 0, s>>>(a.idx, nnz, old_to_new, idx2);
@@ -1120,21 +1123,41 @@ int build_lav_staged(const CsrView& a, int dtype, float dense_frac, SegCsr** out
         cudaFree(tmp);
         cudaFree(stmp);
     }
-    long long dense_cols = 0;
-    GBK_CUDA(cudaMemcpyAsync(&dense_cols, thr, 8, cudaMemcpyDeviceToHost, s));
+    long long dc = 0;
+    GBK_CUDA(cudaMemcpyAsync(&dc, thr, 8, cudaMemcpyDeviceToHost, s));
     GBK_CUDA(cudaStreamSynchronize(s));
-    f->dense_cols = dense_cols;
-    CsrView r = a;  // same rows and values, relabelled columns
-    r.idx = idx2;
-    r.bins = nullptr;
-    int rc = build_segsmem(r, dtype, &f->staged, s);
     cudaFree(cdeg);
     cudaFree(cdeg_sorted);
     cudaFree(iota);
     cudaFree(old_to_new);
-    cudaFree(idx2);
     cudaFree(acc);
     cudaFree(thr);
+    *new_to_old = n2o;
+    *idx_out = idx2;
+    if (dense_cols) *dense_cols = dc;
+    return GBK_SUCCESS;
+}
+
+namespace {
+
+int build_lav_staged(const CsrView& a, int dtype, float dense_frac, SegCsr** out, cudaStream_t s) {
+    const int64_t nc = a.ncols;
+    SegCsr* f = new SegCsr();
+    f->n = a.nrows;
+    f->ncols = nc;
+    const size_t eb = dtype == GBK_F32 ? sizeof(float) : sizeof(int32_t);
+    GBK_CUDA(cudaMalloc(&f->xr, eb * (nc > 0 ? nc : 1)));
+    int32_t* idx2 = nullptr;
+    int rc = indegree_order(a, dense_frac, &f->col_new_to_old, &idx2, &f->dense_cols, s);
+    if (rc) {
+        free_seg(f);
+        return rc;
+    }
+    CsrView r = a;  // same rows and values, relabelled columns
+    r.idx = idx2;
+    r.bins = nullptr;
+    rc = build_segsmem(r, dtype, &f->staged, s);
+    cudaFree(idx2);
     if (rc) {
         free_seg(f);
         return rc;
@@ -1292,6 +1315,11 @@ int format_dispatch(gbk_matrix A, int orient, int sr, int accum, const T* x, T* 
 int spmv_format(gbk_matrix A, int transpose, int sr, int accum, int dtype, const void* x, void* y,
                 cudaStream_t s) {
     const int orient = transpose ? 1 : 0;
+    if (A->format == GBK_FMT_SELL_C && A->sellw[orient]) {
+        const int rc = run_sellw(A->sellw[orient], sr, accum, dtype, x, y, s);
+        if (rc != GBK_UNSUPPORTED) return rc;
+        return spmv_csr(orient ? A->csc : A->csr, sr, accum, dtype, x, y, nullptr, 0, 0, s);
+    }
     if (A->format == GBK_FMT_CSR_SEG && A->segx[orient]) {
         const int rc = run_segsmem(A->segx[orient], sr, accum, dtype, x, y, s);
         if (rc != GBK_UNSUPPORTED) return rc;
@@ -1309,6 +1337,8 @@ int free_formats(gbk_matrix A) {
         free_seg(A->lav[o]);
         free_segsmem(A->segx[o]);
         A->segx[o] = nullptr;
+        free_sellw(A->sellw[o]);
+        A->sellw[o] = nullptr;
         A->sell[o] = nullptr;
         A->seg[o] = nullptr;
         A->lav[o] = nullptr;
@@ -1346,7 +1376,9 @@ int build_format(gbk_matrix A, gbk_format fmt, const gbk_format_params* p, cudaS
     if (rc) return rc;
     for (int o = 0; o < 2; o++) {
         const CsrView& v = o ? A->csc : A->csr;
-        if (fmt == GBK_FMT_SELL_C) {
+        if (fmt == GBK_FMT_SELL_C && prm.seg_staged == 1) {
+            rc = build_sellw(v, A->vtype, prm.sell_reorder_cols != 0, &A->sellw[o], s);
+        } else if (fmt == GBK_FMT_SELL_C) {
             rc = A->vtype == GBK_F32
                      ? build_sell<float>(v, prm.sell_sigma, prm.sell_hot_cols, prm.sell_reorder_cols, &A->sell[o], s)
                      : build_sell<int32_t>(v, prm.sell_sigma, prm.sell_hot_cols, prm.sell_reorder_cols, &A->sell[o],
@@ -1378,6 +1410,7 @@ size_t format_bytes(gbk_matrix A) {
             b += f->ov.nnz * (4 + eb) + (f->ov.nrows + 1) * 4;
         }
         b += segsmem_bytes(A->segx[o]);
+        b += sellw_bytes(A->sellw[o]);
         const SegCsr* g = A->seg[o] ? A->seg[o] : A->lav[o];
         if (g && g->staged) b += segsmem_bytes(g->staged) + g->ncols * (4 + eb);
         else if (g) b += g->v.nnz * (4 + eb) + (g->nvrows + 1) * 4 * 2 + (g->n + 1) * 4 + g->nvrows * eb;
@@ -1387,6 +1420,7 @@ size_t format_bytes(gbk_matrix A) {
 
 int64_t format_padded_nnz(gbk_matrix A) {
     if (A->format == GBK_FMT_SELL_C && A->sell[0]) return A->sell[0]->padded + A->sell[0]->ov.nnz;
+    if (A->format == GBK_FMT_SELL_C && A->sellw[0]) return sellw_padded(A->sellw[0]);
     return A->csr.nnz;
 }
 

@@ -132,26 +132,6 @@ __global__ void k_ss_cvr(const int32_t* __restrict__ vid, int64_t nnz, int64_t n
     cvr[q] = vid[min(q * kChunk, nnz)] - 1;
 }
 
-__device__ __forceinline__ void atomic_min_any(float* p, float v) {
-    // order-preserving on the bit patterns: non-negative floats order as ints,
-    // negative ones in reverse as unsigned ints
-    if (v >= 0.0f)
-        atomicMin((int*)p, __float_as_int(v));
-    else
-        atomicMax((unsigned int*)p, __float_as_uint(v));
-}
-__device__ __forceinline__ void atomic_min_any(int32_t* p, int32_t v) { atomicMin(p, v); }
-
-__device__ __forceinline__ void atomic_add_any(float* p, float v) { atomicAdd(p, v); }
-__device__ __forceinline__ void atomic_add_any(int32_t* p, int32_t v) {
-    // saturating, like elem_add, so INT_MAX stays the min-plus infinity
-    int old = *((volatile int*)p), assumed;
-    do {
-        assumed = old;
-        old = atomicCAS(p, assumed, elem_add(assumed, v));
-    } while (old != assumed);
-}
-
 template <int SR>
 struct AddClass {  // 0 plus, 1 min, 2 or, -1 not folded atomically
     static constexpr int value = (SR == GBK_PLUS_TIMES || SR == GBK_PLUS_SECOND || SR == GBK_PLUS_ONE) ? 0

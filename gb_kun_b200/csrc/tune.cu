@@ -24,6 +24,7 @@ struct Candidate {
     int32_t sigma;
     int32_t kernel;
     int32_t hot;
+    int32_t staged;  // SELL-C: 1 = inside staged x windows (hot == -1 then renumbers the columns first)
 };
 
 // Order matches gbk_tune_result.candidate_ms (include/gbk.h).
@@ -34,6 +35,7 @@ const Candidate kCandidates[] = {
     {GBK_FMT_LAV, 0, kKernelAuto, 0},        {GBK_FMT_SELL_C, 4096, kKernelAuto, 16384},
     {GBK_FMT_SELL_C, 4096, kKernelAuto, 53248}, {GBK_FMT_SELL_C, 256, kKernelAuto, 53248},
     {GBK_FMT_SELL_C, 4096, kKernelAuto, -1},    {GBK_FMT_SELL_C, 256, kKernelAuto, -1},
+    {GBK_FMT_SELL_C, 0, kKernelAuto, 0, 1},     {GBK_FMT_SELL_C, 0, kKernelAuto, -1, 1},
 };
 constexpr int kNumCandidates = sizeof(kCandidates) / sizeof(kCandidates[0]);
 
@@ -100,7 +102,9 @@ int apply_candidate(gbk_matrix A, const Candidate& c, cudaStream_t s) {
     p.sell_sigma = c.sigma ? c.sigma : 4096;
     p.csr_kernel = c.kernel;
     p.sell_hot_cols = c.hot > 0 ? c.hot : 0;
-    p.sell_reorder_cols = c.hot < 0 ? 1 : 0;  // hot == -1: renumbered columns, no staging
+    p.sell_reorder_cols = c.hot < 0 ? 1 : 0;  // hot == -1: renumbered columns
+    if (c.fmt == GBK_FMT_SELL_C) p.seg_staged = c.staged;
+    else if (p.seg_staged > 0) p.seg_staged = 0;
     return build_format(A, c.fmt, &p, s);
 }
 
@@ -182,7 +186,8 @@ extern "C" int gbk_matrix_autotune(gbk_matrix A, int transpose, gbk_semiring sr,
     res.format = kCandidates[best].fmt;
     res.sell_sigma = kCandidates[best].sigma;
     res.csr_kernel = kCandidates[best].kernel;
-    res.sell_hot_cols = kCandidates[best].hot;  // -1: columns renumbered, x not staged
+    res.sell_hot_cols = kCandidates[best].hot;  // -1: columns renumbered
+    res.sell_staged = kCandidates[best].staged;
     res.best_ms = res.cached ? 0.0f : res.candidate_ms[best];
     if (result) *result = res;
     return GBK_SUCCESS;

@@ -39,9 +39,13 @@ typedef struct gbk_format_params {
                                 0 = off; at most 53248 */
     int32_t sell_reorder_cols; /* SELL-C: renumber columns by in-degree (most used first) so gathers of
                                   popular x values share sectors and L1 lines; implied by sell_hot_cols */
-    int32_t seg_staged;      /* CSR_SEG: 0 (default) windows of 49152 columns whose x values are staged in
-                                shared memory, row sums folded into y atomically; -1 = seg_cols-wide
-                                segments gathered from L2 and merged per row in segment order */
+    int32_t seg_staged;      /* CSR_SEG / LAV: 0 (default) windows of 49152 columns whose x values are
+                                staged in shared memory, row sums folded into y atomically; -1 =
+                                seg_cols-wide segments gathered from L2 and merged per row in segment
+                                order.  SELL-C: 1 = SELL-C-sigma built inside staged windows of 49152
+                                columns (sigma = the window, virtual rows in pieces of at most 32 entries;
+                                sell_reorder_cols renumbers the columns by in-degree first); 0 (default)
+                                = the gathered SELL-C */
 } gbk_format_params;
 
 /* A mask argument: either dense (n entries of `dtype`, non-zero = set) or
@@ -101,10 +105,12 @@ typedef struct gbk_tune_result {
     int32_t cached;          /* 1 when the choice came from the cache (nothing was timed) */
     int32_t ncandidates;
     float best_ms;
-    float candidate_ms[12];  /* CSR bins, CSR merge-path, SELL-C sigma 1 / 256 / 4096, CSR_SEG, LAV,
+    float candidate_ms[16];  /* CSR bins, CSR merge-path, SELL-C sigma 1 / 256 / 4096, CSR_SEG, LAV,
                                 SELL-C sigma 4096 with 16384 / 53248 hot columns, sigma 256 with 53248,
-                                SELL-C sigma 4096 / 256 with renumbered columns */
-    int32_t sell_hot_cols;   /* chosen hot-column count (SELL-C only; -1 = renumbered columns only) */
+                                SELL-C sigma 4096 / 256 with renumbered columns, SELL-C in staged x
+                                windows without / with renumbered columns; unused entries 0 */
+    int32_t sell_hot_cols;   /* chosen hot-column count (SELL-C only; -1 = renumbered columns) */
+    int32_t sell_staged;     /* 1 when the chosen SELL-C runs inside staged x windows */
 } gbk_tune_result;
 
 /* Per-graph autotuner (no counterpart in the reference, which takes the

@@ -36,7 +36,7 @@ GRAPHS = {
 }
 
 FORMATS = [("SELL_C", 1), ("SELL_C", 256), ("SELL_C", 4096), ("SELL_C_HOT", 4096), ("SELL_C_HOT", 1), ("CSR_SEG", 0),
-           ("CSR_SEG_MERGE", 0), ("LAV", 0)]
+           ("CSR_SEG_MERGE", 0), ("LAV", 0), ("SELL_C_STAGED", 0), ("SELL_C_STAGED", 1)]
 
 
 def apply(A, fmt, sigma, seg_cols):
@@ -44,6 +44,8 @@ def apply(A, fmt, sigma, seg_cols):
     staged-window kernel, CSR_SEG_MERGE the unstaged segments with a merge."""
     if fmt == "SELL_C_HOT":
         A.set_format("SELL_C", sigma=sigma, hot_cols=1024)
+    elif fmt == "SELL_C_STAGED":
+        A.set_format("SELL_C", seg_staged=1, reorder_cols=sigma)  # sigma column: 1 = renumber columns
     elif fmt == "CSR_SEG_MERGE":
         A.set_format("CSR_SEG", seg_cols=seg_cols, seg_staged=-1)
     else:
@@ -131,11 +133,12 @@ def test_masked_call_uses_csr_semantics(capi, oracle):
     assert np.array_equal(y.cpu().numpy(), oracle.mxv("lor_land", g, val, x, y0, mask=m, mask_mode=5))
 
 
-@pytest.mark.parametrize("fmt", ["CSR_SEG", "LAV"])
+@pytest.mark.parametrize("fmt", ["CSR_SEG", "LAV", "SELL_C_STAGED", "SELL_C_STAGED_REORDER"])
 @pytest.mark.parametrize("sr", ["plus_times", "min_plus", "lor_land", "plus_one", "min_second", "first_wins"])
 @pytest.mark.parametrize("accum", ["second", "plus"])
 def test_staged_segments_many_windows(capi, oracle, fmt, sr, accum):
-    """CSR_SEG, and LAV (columns renumbered by in-degree on the device), with
+    """CSR_SEG, LAV (columns renumbered by in-degree on the device) and
+    SELL-C-sigma inside windows (columns in their order or renumbered), with
     x windows in shared memory on a graph of 3 windows (131072 columns),
     every add class (atomic add / min / or) and the CSR fallback for a
     non-associative add; float sums within REL_L1_TOL, integers exact."""
@@ -150,7 +153,10 @@ def test_staged_segments_many_windows(capi, oracle, fmt, sr, accum):
         x[::5] = 0
         y0 = np.full(g.n, 7, np.int32)
     A = capi.Matrix.from_graph(g, val)
-    A.set_format(fmt)
+    if fmt.startswith("SELL_C_STAGED"):
+        A.set_format("SELL_C", seg_staged=1, reorder_cols=int(fmt.endswith("REORDER")))
+    else:
+        A.set_format(fmt)
     for transpose in (False, True):
         y = dev(y0.copy())
         A.mxv(dev(x), y, semiring=sr, accum=accum, transpose=transpose)
@@ -182,3 +188,27 @@ def test_lav_renumbering_matches_reference_order(capi, oracle):
         A.mxv(dev(x), y, semiring="min_plus")
         outs.append(y.cpu().numpy())
     assert np.array_equal(outs[0], want) and np.array_equal(outs[1], want)
+
+
+def test_staged_sell_long_rows_and_pieces(capi, oracle):
+    """Staged SELL-C on a hub graph: virtual rows longer than 32 entries are
+    cut into pieces, every piece folds into its row; plus-times within
+    REL_L1_TOL, min-plus exact; accumulate into a non-zero y."""
+    g = hub_graph()
+    for reorder in (0, 1):
+        val = gg.values_f32(g, seed=5)
+        x = gg.vector_f32(g.n, seed=6)
+        A = capi.Matrix.from_graph(g, val)
+        A.set_format("SELL_C", seg_staged=1, reorder_cols=reorder)
+        assert A.info().padded_nnz >= g.nnz
+        y = dev(np.full(g.n, 0.25, np.float32))
+        A.mxv(dev(x), y, accum="plus")
+        assert rel_l1(y.cpu().numpy(), 0.25 + oracle.spmv_f64(g, val, x)) < REL_L1_TOL
+        vi = gg.weights_i32(g, seed=7, lo=1, hi=90)
+        xi = (gg.vector_f32(g.n, seed=8) * 500).astype(np.int32)
+        B = capi.Matrix.from_graph(g, vi)
+        B.set_format("SELL_C", seg_staged=1, reorder_cols=reorder)
+        y0 = np.full(g.n, 3, np.int32)
+        yi = dev(y0.copy())
+        B.mxv(dev(xi), yi, semiring="min_plus", accum="min")
+        assert np.array_equal(yi.cpu().numpy(), oracle.mxv("min_plus", g, vi, xi, y0, accum=6))

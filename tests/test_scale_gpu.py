@@ -100,6 +100,8 @@ SWEEP = [
     ("SELL_C_s256", dict(fmt="SELL_C", sigma=256)),
     ("SELL_C_s4096", dict(fmt="SELL_C", sigma=4096)),
     ("SELL_C_s4096_reorder", dict(fmt="SELL_C", sigma=4096, reorder_cols=1)),
+    ("SELL_C_staged", dict(fmt="SELL_C", seg_staged=1)),
+    ("SELL_C_staged_reorder", dict(fmt="SELL_C", seg_staged=1, reorder_cols=1)),
     ("CSR_SEG", dict(fmt="CSR_SEG")),
     ("CSR_SEG_merge", dict(fmt="CSR_SEG", seg_staged=-1)),
     ("LAV", dict(fmt="LAV")),
