@@ -724,6 +724,8 @@ def run_serve(args):
     G = lc.Graph(g, weights=w)
     G.bfs(int(cand[0]))
     plain_bfs = statistics.median([G.bfs(int(s))[1] for s in cand[1:6]])
+    G.bfs_ops(int(cand[0]))
+    plain_bfs_ops = statistics.median([G.bfs_ops(int(s))[1] for s in cand[1:6]])
     plain_sssp = statistics.median([G.sssp_i32(int(s))[1] for s in cand[1:4]])
     G.ppr(int(cand[0]))
     plain_ppr = statistics.median([G.ppr(int(s))[2] for s in cand[1:4]])
@@ -755,7 +757,8 @@ def run_serve(args):
         "batches": nb, "device_bytes_used": used, "memory_budget": budget,
         "one_at_a_time": {"qps_poisson": round(m / wall1, 2), "qps_capacity": round(cap1, 2),
                           "latency_ms": latency_stats(res1), "queries": m,
-                          "service_ms_engine": ser, "service_ms_plain_lablas": {"bfs": plain_bfs, "sssp": plain_sssp, "ppr": plain_ppr},
+                          "service_ms_engine": ser, "service_ms_plain_lablas": {"bfs": plain_bfs, "bfs_graphblas_calls": plain_bfs_ops,
+                                                      "sssp": plain_sssp, "ppr": plain_ppr},
                           "qps_capacity_best_single_query_path": round(one_best_qps, 2)},
         "speedup_qps_vs_one_at_a_time": round(cap / max(cap1, one_best_qps), 2),
         "e2e": {"value": round(qps, 2), "unit": "queries/s", "h2d_bytes_per_step": 0,
@@ -838,10 +841,19 @@ def run_algorithms(args, light=False):
     lv, ms = twice(lambda: G.bfs(int(src[1])))
     ref = R.bfs(g, int(src[1])) if R else (None, None)
     teps = int(degs[lv > 0].sum()) / (ms * 1e-3) / 1e9
-    rec("bfs", ms, ref[1], None if ref[0] is None else bool(np.array_equal(lv, ref[0])), {"gteps": round(teps, 3)})
+    rec("bfs", ms, ref[1], None if ref[0] is None else bool(np.array_equal(lv, ref[0])),
+        {"gteps": round(teps, 3), "path": "gbk_bfs_levels: level loop on the device, one graph launch"})
+    lv2, ms2 = twice(lambda: G.bfs_ops(int(src[1])))
+    rec("bfs_graphblas_calls", ms2, ref[1], None if ref[0] is None else bool(np.array_equal(lv2, ref[0])),
+        {"gteps": round(int(degs[lv2 > 0].sum()) / (ms2 * 1e-3) / 1e9, 3),
+         "path": "bfs_blast's assign / masked vxm / reduce per level, a host read per level"})
     lab, ms = twice(G.cc)
     ref = R.cc(g) if R else (None, None)
-    rec("cc", ms, ref[1], None if ref[0] is None else bool(np.array_equal(lab, ref[0])))
+    rec("cc", ms, ref[1], None if ref[0] is None else bool(np.array_equal(lab, ref[0])),
+        {"path": "gbk_cc_labels: union-find, three launches"})
+    lab2, it2, ms2 = twice(G.cc_fastsv)
+    rec("cc_fastsv_calls", ms2, ref[1], None if ref[0] is None else bool(np.array_equal(lab2, ref[0])),
+        {"iterations": it2, "path": "cc.hpp's FastSV GraphBLAS calls, a host read per iteration"})
     d, ms = twice(lambda: G.sssp_f32(int(src[2])))
     ref = R.sssp(g, w, int(src[2])) if R else (None, None)
     rec("sssp", ms, ref[1], None if ref[0] is None else bool(np.array_equal(d, ref[0])))

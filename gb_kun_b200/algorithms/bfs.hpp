@@ -1,9 +1,16 @@
-// Level-synchronous BFS through the lablas:: API, the GraphBLAST "blast"
-// formulation of algorithms/bfs/bfs.hpp:93-142: levels start at 1 for the
-// source, 0 marks unvisited; each level assigns the frontier's level, then
-// expands the frontier with an or-and vxm masked by the complement of the
-// visited set.  A sparse frontier is pushed (SpMSpV over the CSR), a dense
-// one pulled (masked SpMV over the CSC), as backend::vxm decides.
+// Level-synchronous BFS through the lablas:: API with the result of the
+// GraphBLAST "blast" formulation of algorithms/bfs/bfs.hpp:94-142: levels
+// start at 1 for the source, 0 marks unvisited, edges are followed along the
+// rows of A.
+//
+//  * bfs_blast runs the whole level loop on the device (gbk_bfs_levels:
+//    direction-optimising, one CUDA graph launch per search).
+//  * bfs_blast_ops is the reference's own sequence of GraphBLAS calls: each
+//    level assigns the frontier's level, then expands the frontier with an
+//    or-and vxm masked by the complement of the visited set (a sparse
+//    frontier pushed through SpMSpV over the CSR, a dense one pulled through
+//    a masked SpMV over the CSC, as backend::vxm decides) and reads the
+//    frontier's size back to the host.
 #pragma once
 
 #include "lablas/gb_kun.h"
@@ -13,6 +20,13 @@ namespace algorithm {
 
 template <typename T>
 void bfs_blast(Vector<T>* v, const Matrix<T>* A, Index s, Descriptor* desc) {
+    (void)desc;
+    throw_if(gbk_bfs_levels(A->handle(), (int64_t)s, 0, Vector<T>::dtype, v->dense_ptr(), nullptr, stream()),
+             "bfs_blast");
+}
+
+template <typename T>
+void bfs_blast_ops(Vector<T>* v, const Matrix<T>* A, Index s, Descriptor* desc) {
     const Index n = A->nrows();
     v->fill((T)0);
     Vector<T> f1(n);

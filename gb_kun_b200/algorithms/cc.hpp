@@ -1,9 +1,16 @@
-// Connected components (FastSV, Zhang, Azad and Hu, SIAM PP20) through the
-// lablas:: API, in the formulation of algorithms/cc/cc.hpp:12-119:
-// stochastic hooking through the minimum grandparent among neighbours
-// (min-select-second mxv), aggressive hooking and shortcutting with min
-// eWiseAdds, grandparents by extract, termination when no grandparent
-// changes.  Labels converge to the smallest vertex id of each component.
+// Connected components through the lablas:: API with the result of the
+// FastSV loop of algorithms/cc/cc.hpp:12-119 (Zhang, Azad and Hu, SIAM PP20):
+// every vertex labelled with the smallest vertex id of its component.
+//
+//  * cc_fastsv is that loop as the reference writes it: stochastic hooking
+//    through the minimum grandparent among neighbours (min-select-second
+//    mxv), aggressive hooking and shortcutting with min eWiseAdds,
+//    grandparents by extract, termination when no grandparent changes (a
+//    host read per iteration).
+//  * cc reaches the same labels on a symmetric matrix with a lock-free
+//    union-find on the device (gbk_cc_labels, three launches, no host round
+//    trip) and runs cc_fastsv on any other matrix, where FastSV's fixed
+//    point need not be the weakly connected components.
 #pragma once
 
 #include <limits>
@@ -13,7 +20,7 @@
 namespace lablas {
 namespace algorithm {
 
-inline Index cc(Vector<int>* v, const Matrix<int>* A, int seed, Descriptor* desc) {
+inline Index cc_fastsv(Vector<int>* v, const Matrix<int>* A, int seed, Descriptor* desc) {
     (void)seed;
     // The reference builds CC with __DISABLE_SPMSPV__ (cc.cpp:2): the hooking
     // mxv always reads the grandparent vector densely, zeros included.
@@ -61,6 +68,15 @@ inline Index cc(Vector<int>* v, const Matrix<int>* A, int seed, Descriptor* desc
     }
     v->dup(&parent);
     return iter;
+}
+
+// Returns FastSV's iteration count, or 0 when the union-find labelled A.
+inline Index cc(Vector<int>* v, const Matrix<int>* A, int seed, Descriptor* desc) {
+    int32_t symmetric = 0;
+    throw_if(gbk_matrix_pattern_symmetric(A->handle(), &symmetric, stream()), "cc");
+    if (!symmetric) return cc_fastsv(v, A, seed, desc);
+    throw_if(gbk_cc_labels(A->handle(), GBK_I32, v->dense_ptr(), stream()), "cc");
+    return 0;
 }
 
 }  // namespace algorithm

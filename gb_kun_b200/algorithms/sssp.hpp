@@ -1,11 +1,18 @@
-// Bellman-Ford SSSP through the lablas:: API, the formulation of
-// algorithms/sssp/sssp_blast.hpp:8-72: every round relaxes all edges out of
-// the current distance vector with a min-plus vxm, records which vertices
-// improved (custom-less eWiseAdd), keeps the minimum and stops when no
-// vertex improves.  Distances start at the type's maximum ("infinity") with
-// 0 at the source.  T = float restates the reference exactly (integer
-// weights below 2^24 are exact in float); T = int runs the same rounds with
-// int32 weights and saturating additions.
+// Bellman-Ford SSSP through the lablas:: API with the distances of
+// algorithms/sssp/sssp_blast.hpp:8-72: distances start at the type's maximum
+// ("infinity") with 0 at the source; T = float restates the reference exactly
+// (integer weights below 2^24 are exact in float); T = int runs with int32
+// weights and saturating additions.
+//
+//  * sssp_bellman_ford_blast runs a label-correcting worklist on the device
+//    (gbk_sssp_dist, one graph launch for all rounds).  Each distance is the
+//    minimum over walks of the left-to-right rounded sums either way, since
+//    rounding is monotone, so the result equals the reference's.
+//  * sssp_bellman_ford_blast_ops is the reference's own sequence: every
+//    round relaxes all edges out of the current frontier vector with a
+//    min-plus vxm, records which vertices improved (custom-less eWiseAdd),
+//    keeps the minimum and stops when no vertex improves (a host read per
+//    round).
 #pragma once
 
 #include <limits>
@@ -15,8 +22,17 @@
 namespace lablas {
 namespace algorithm {
 
+// Returns the worklist rounds run.
 template <typename T>
 Index sssp_bellman_ford_blast(Vector<T>* v, const Matrix<T>* A, Index s, Descriptor* desc) {
+    (void)desc;
+    int32_t rounds = 0;
+    throw_if(gbk_sssp_dist(A->handle(), (int64_t)s, v->dense_ptr(), &rounds, stream()), "sssp_bellman_ford_blast");
+    return rounds;
+}
+
+template <typename T>
+Index sssp_bellman_ford_blast_ops(Vector<T>* v, const Matrix<T>* A, Index s, Descriptor* desc) {
     const Index n = A->nrows();
     const T inf = std::numeric_limits<T>::max();
     v->fill(inf);

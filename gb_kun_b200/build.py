@@ -38,6 +38,7 @@ CU_SOURCES = [
     "spmv_sellw.cu",
     "spmspv.cu",
     "spmspv_sparse.cu",
+    "single.cu",
     "vector_ops.cu",
     "spgemm.cu",
     "tune.cu",

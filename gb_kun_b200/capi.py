@@ -133,6 +133,10 @@ def _declare(lib):
         "gbk_msbfs": ([vp, vp, ci, vp, ci, vp, vp], ci),
         "gbk_ppr": ([vp, vp, ci, C.c_double, C.c_double, ci, vp, vp, vp], ci),
         "gbk_sssp_multi": ([vp, vp, ci, vp, vp, vp], ci),
+        "gbk_bfs_levels": ([vp, i64, ci, ci, vp, C.POINTER(i32), vp], ci),
+        "gbk_matrix_pattern_symmetric": ([vp, C.POINTER(i32), vp], ci),
+        "gbk_cc_labels": ([vp, ci, vp, vp], ci),
+        "gbk_sssp_dist": ([vp, i64, vp, C.POINTER(i32), vp], ci),
         "gbk_batch_autotune": ([vp, ci, vp, ci, C.POINTER(BatchTuneResult), vp], ci),
         "gbk_mxm": ([C.POINTER(vp), vp, vp, ci, vp], ci),
         "gbk_triangle_count": ([vp, C.POINTER(C.c_uint64), vp], ci),
@@ -381,6 +385,35 @@ class Matrix:
         check(lib().gbk_msbfs(self.h, ptr(src), len(src), ptr(levels), int(direction), ptr(depths),
                               stream_ptr(stream)), "gbk_msbfs")
         return depths
+
+    def bfs(self, source, levels, direction=0, stream=None):
+        """Single-source BFS levels into levels (device, n elements of int32, int64, float32 or
+        float64; source 1, unreached 0).  direction: 0 switches between top-down and bottom-up
+        per level, 1 top-down only, 2 bottom-up only.  Returns the largest level."""
+        depth = C.c_int32(0)
+        check(lib().gbk_bfs_levels(self.h, int(source), int(direction), dtype_code(levels), ptr(levels),
+                                   C.byref(depth), stream_ptr(stream)), "gbk_bfs_levels")
+        return depth.value
+
+    def sssp(self, source, dist, stream=None):
+        """Shortest-path distances from source into dist (device, n elements of the matrix's value
+        type: float32 with FLT_MAX or int32 with INT32_MAX for unreachable).  Returns the rounds run."""
+        rounds = C.c_int32(0)
+        check(lib().gbk_sssp_dist(self.h, int(source), ptr(dist), C.byref(rounds), stream_ptr(stream)),
+              "gbk_sssp_dist")
+        return rounds.value
+
+    def pattern_symmetric(self, stream=None) -> bool:
+        """True when the matrix equals its transpose in pattern (rows sorted)."""
+        out = C.c_int32(0)
+        check(lib().gbk_matrix_pattern_symmetric(self.h, C.byref(out), stream_ptr(stream)),
+              "gbk_matrix_pattern_symmetric")
+        return bool(out.value)
+
+    def cc(self, labels, stream=None):
+        """Connected-component labels (smallest vertex id per component) into labels (device, n
+        elements of int32, int64 or float32)."""
+        check(lib().gbk_cc_labels(self.h, dtype_code(labels), ptr(labels), stream_ptr(stream)), "gbk_cc_labels")
 
     def ppr(self, seeds, ranks, damping=0.85, tol=1e-6, itermax=100, stream=None):
         """Personalised PageRank for up to 32 seeds into ranks (device float32, len(seeds) x n).

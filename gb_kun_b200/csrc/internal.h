@@ -61,6 +61,7 @@ struct gbk_matrix_s {
     gbk::CsrView csr;           // A
     gbk::CsrView csc;           // A^T (built lazily)
     bool has_csc = false;
+    int8_t pattern_symmetric = -1;  // -1 unknown; gbk_matrix_pattern_symmetric
     gbk_format format = GBK_FMT_CSR;
     gbk_format_params params{};
     gbk::SellC* sell[2] = {nullptr, nullptr};

@@ -164,6 +164,20 @@ int gbk_lablas_bfs(gbk_lablas_graph g, int64_t source, int32_t* levels, double* 
     });
 }
 
+int gbk_lablas_bfs_ops(gbk_lablas_graph g, int64_t source, int32_t* levels, double* ms) {
+    if (!g || !levels) return GBK_NULL_POINTER;
+    return guarded([&] {
+        auto* A = g->unit_f();
+        lablas::Vector<float> lv(g->n);
+        lablas::Descriptor desc;
+        Timer t(ms);
+        lablas::algorithm::bfs_blast_ops(&lv, A, (Index)source, &desc);
+        t.stop();
+        copy_out(lv, levels);
+        return 0;
+    });
+}
+
 int gbk_lablas_cc(gbk_lablas_graph g, int32_t* labels, int32_t* iterations, double* ms) {
     if (!g || !labels) return GBK_NULL_POINTER;
     return guarded([&] {
@@ -179,6 +193,21 @@ int gbk_lablas_cc(gbk_lablas_graph g, int32_t* labels, int32_t* iterations, doub
     });
 }
 
+int gbk_lablas_cc_fastsv(gbk_lablas_graph g, int32_t* labels, int32_t* iterations, double* ms) {
+    if (!g || !labels) return GBK_NULL_POINTER;
+    return guarded([&] {
+        auto* A = g->unit_i();
+        lablas::Vector<int> comp(g->n);
+        lablas::Descriptor desc;
+        Timer t(ms);
+        Index it = lablas::algorithm::cc_fastsv(&comp, A, 0, &desc);
+        t.stop();
+        if (iterations) *iterations = (int32_t)it;
+        copy_out(comp, labels);
+        return 0;
+    });
+}
+
 int gbk_lablas_sssp_f32(gbk_lablas_graph g, int64_t source, float* dist, double* ms) {
     if (!g || !dist) return GBK_NULL_POINTER;
     return guarded([&] {
@@ -187,6 +216,20 @@ int gbk_lablas_sssp_f32(gbk_lablas_graph g, int64_t source, float* dist, double*
         lablas::Descriptor desc;
         Timer t(ms);
         lablas::algorithm::sssp_bellman_ford_blast(&d, A, (Index)source, &desc);
+        t.stop();
+        copy_out(d, dist);
+        return 0;
+    });
+}
+
+int gbk_lablas_sssp_f32_ops(gbk_lablas_graph g, int64_t source, float* dist, double* ms) {
+    if (!g || !dist) return GBK_NULL_POINTER;
+    return guarded([&] {
+        auto* A = g->weights_f();
+        lablas::Vector<float> d(g->n);
+        lablas::Descriptor desc;
+        Timer t(ms);
+        lablas::algorithm::sssp_bellman_ford_blast_ops(&d, A, (Index)source, &desc);
         t.stop();
         copy_out(d, dist);
         return 0;

@@ -1,0 +1,828 @@
+// Single-query traversals with the whole iteration loop on the device.
+//
+// The reference runs its algorithms as one GraphBLAS call per step with a
+// host read of the convergence scalar every iteration (bfs_blast,
+// algorithms/bfs/bfs.hpp:94-142; sssp_bellman_ford_blast,
+// algorithms/sssp/sssp_blast.hpp:8-72; cc, algorithms/cc/cc.hpp:12-119); the
+// drop-in header runs exactly that sequence.  These entry points compute the
+// same outputs with fused device loops:
+//
+//  * gbk_bfs_levels: direction-optimising BFS along CSR rows (the vxm of
+//    bfs_blast), levels 1 for the source, k + 1 at distance k, 0 unreached.
+//    Each level expands the frontier top-down from a queue of its vertices
+//    or bottom-up over the unvisited vertices' in-edges (CSC) testing a
+//    frontier bitmap, and records every vertex it reaches in both the next
+//    queue and the next bitmap, so switching direction needs no conversion.
+//    A one-warp control kernel switches on the frontier's out-edges against
+//    the unvisited vertices' out-edges (Beamer's rule) and ends the loop;
+//    the level's kernels form the body of one CUDA graph whose `while` node
+//    the control kernel drives, so a whole BFS is one graph launch.
+//  * gbk_sssp_dist: the distances of sssp_bellman_ford_blast by a
+//    label-correcting worklist: each round relaxes the out-edges of the
+//    vertices whose distance dropped in the round before (an atomic min per
+//    edge, a bitmap so each improved vertex is queued once), one graph
+//    launch for all rounds.
+//  * gbk_cc_labels: connected components as min-vertex-id labels (the fixed
+//    point FastSV reaches on an undirected graph) by lock-free union-find
+//    with sampled linking (Sutton, Ben-Nun and Barak, "Optimizing Parallel
+//    Graph Connectivity Computation via Subgraph Sampling", IPDPS 2018):
+//    every vertex first links along its first two entries, the largest
+//    component is found from a sample of 1024 vertices, and only vertices
+//    outside it link along their remaining entries (on a symmetric pattern
+//    the other end of every skipped edge links it).  Links always put the
+//    larger of two roots under the smaller one (compare-and-swap), so a
+//    component's root is its smallest vertex and the labels do not depend
+//    on the order of the links.  A non-symmetric pattern links every entry
+//    in both directions, which gives its weakly connected components.
+//
+// Frontier expansion is load-balanced the same way for BFS and SSSP: a warp
+// takes 32 frontier vertices; rows under kHeavy entries are spread over the
+// warp's lanes edge by edge (a warp scan of their lengths and a 5-step
+// search for each lane's row), longer rows are cut into kChunk-entry chunks
+// that a second kernel of the same level hands out one per warp.
+#include <algorithm>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace gbk {
+
+namespace {
+
+constexpr int kT = 256;
+constexpr unsigned kAll = 0xffffffffu;
+constexpr int kHeavy = 32;   // rows with at least this many entries are cut into chunks
+constexpr int kChunk = 256;  // entries per chunk
+
+int blocks_for_sm(const void* kern) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kT, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    return per_sm * num_sms();
+}
+
+unsigned grid1(int64_t n) { return (unsigned)std::max<int64_t>(1, (n + kT - 1) / kT); }
+
+// A graph whose root is a `while` node around the kernels `body` launches on
+// the stream it is given (captured once; the last of them sets the
+// condition from the device).
+template <typename Body>
+int build_loop_graph(cudaGraph_t* graph, cudaGraphExec_t* exec, Body body) {
+    GBK_CUDA(cudaGraphCreate(graph, 0));
+    cudaGraphConditionalHandle handle;
+    GBK_CUDA(cudaGraphConditionalHandleCreate(&handle, *graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = handle;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    GBK_CUDA(cudaGraphAddNode(&node, *graph, nullptr, 0, &p));
+    cudaGraph_t bodyg = p.conditional.phGraph_out[0];
+    cudaStream_t cs;
+    GBK_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCaptureToGraph(cs, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(cs);
+        return cuda_fail(e, "cudaStreamBeginCaptureToGraph", __FILE__, __LINE__);
+    }
+    body(cs, handle);
+    cudaError_t le = cudaGetLastError();
+    cudaGraph_t captured = nullptr;
+    e = cudaStreamEndCapture(cs, &captured);
+    cudaStreamDestroy(cs);
+    if (le != cudaSuccess) return cuda_fail(le, "loop body launch", __FILE__, __LINE__);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+    GBK_CUDA(cudaGraphInstantiate(exec, *graph, 0));
+    return GBK_SUCCESS;
+}
+
+// Launches the loop graph once on s and releases it (an executable graph
+// destroyed while it runs is released when it ends).
+template <typename Body>
+int run_loop_graph(cudaStream_t s, Body body) {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int rc = build_loop_graph(&graph, &exec, body);
+    if (rc == GBK_SUCCESS) {
+        cudaError_t e = cudaGraphLaunch(exec, s);
+        if (e != cudaSuccess) rc = cuda_fail(e, "cudaGraphLaunch", __FILE__, __LINE__);
+        count_launch(1);
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+}
+
+// ---- frontier expansion -----------------------------------------------------
+
+struct Chunk {
+    int32_t u;    // the row
+    int32_t beg;  // its entries [beg, min(beg + kChunk, end of row))
+};
+
+__device__ __forceinline__ int32_t warp_incl_scan(int32_t x) {
+    const int lane = threadIdx.x & 31;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(kAll, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+// Appends the lanes with `found` set to q (one atomic per warp).
+__device__ __forceinline__ void queue_append(bool found, int32_t v, int32_t* q, int32_t* count) {
+    const unsigned m = __ballot_sync(kAll, found);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    int32_t base = 0;
+    if (lane == 0) base = atomicAdd(count, __popc(m));
+    base = __shfl_sync(kAll, base, 0);
+    if (found) q[base + __popc(m & ((1u << lane) - 1u))] = v;
+}
+
+// The rows of the frontier qc[0, fc): rows under kHeavy entries edge by edge
+// over the warp's lanes (op.edge(valid, value of the row, entry) on every
+// lane), longer rows appended to `chunks` for expand_heavy.  Op::load(u)
+// gives the per-row value passed to op.edge.
+template <class Op>
+__device__ void expand_light(const int32_t* __restrict__ qc, int32_t fc, const int32_t* __restrict__ rp,
+                             Chunk* __restrict__ chunks, int32_t* nchunks, Op& op) {
+    using V = typename Op::V;
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * kT + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * kT) >> 5;
+    const int64_t ngroups = ((int64_t)fc + 31) / 32;
+    for (int64_t c = gw; c < ngroups; c += nw) {
+        const int64_t k = c * 32 + lane;
+        const int32_t u = k < fc ? qc[k] : -1;
+        const int32_t beg = u >= 0 ? rp[u] : 0, deg = u >= 0 ? rp[u + 1] - beg : 0;
+        const bool heavy = deg >= kHeavy;
+        const int32_t nch = heavy ? (deg + kChunk - 1) / kChunk : 0;
+        const int32_t ich = warp_incl_scan(nch);
+        const int32_t tch = __shfl_sync(kAll, ich, 31);
+        if (tch) {
+            int32_t base = 0;
+            if (lane == 0) base = atomicAdd(nchunks, tch);
+            base = __shfl_sync(kAll, base, 0);
+            for (int32_t i = 0; i < nch; ++i) chunks[base + ich - nch + i] = Chunk{u, beg + i * kChunk};
+        }
+        const int32_t dl = heavy ? 0 : deg;
+        const int32_t incl = warp_incl_scan(dl);
+        const int32_t excl = incl - dl;
+        const int32_t total = __shfl_sync(kAll, incl, 31);
+        const V val = dl > 0 ? op.load(u) : V();
+        for (int32_t t0 = 0; t0 < total; t0 += 32) {
+            const int32_t t = t0 + lane;
+            // the row of edge t: the first lane whose inclusive count exceeds t
+            int j = 0;
+            for (int s = 16; s; s >>= 1)
+                if (__shfl_sync(kAll, incl, j + s - 1) <= t) j += s;
+            j = min(j, 31);  // lanes past the end
+            const int32_t eb = __shfl_sync(kAll, beg, j), ex = __shfl_sync(kAll, excl, j);
+            const V vj = __shfl_sync(kAll, val, j);
+            op.edge(t < total, vj, eb + (t - ex));
+        }
+    }
+}
+
+// The chunks expand_light appended, one warp per chunk.
+template <class Op>
+__device__ void expand_heavy(const Chunk* __restrict__ chunks, int32_t nch, const int32_t* __restrict__ rp, Op& op) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * kT + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * kT) >> 5;
+    for (int64_t c = gw; c < nch; c += nw) {
+        const Chunk ch = chunks[c];
+        const int32_t end = min(ch.beg + kChunk, rp[ch.u + 1]);
+        const typename Op::V val = op.load(ch.u);
+        for (int32_t e0 = ch.beg; e0 < end; e0 += 32) op.edge(e0 + lane < end, val, e0 + lane);
+    }
+}
+
+// Upper bound of the chunks one round appends: every row appears once per
+// round and a row of d >= kHeavy entries gives ceil(d / kChunk) <= d / kHeavy.
+int64_t max_chunks(int64_t nnz) { return nnz / kHeavy + 1; }
+
+// ---- BFS --------------------------------------------------------------------
+
+struct Bfs1State {
+    int32_t level;        // level of the current frontier's vertices
+    int32_t mode;         // 0 top-down (queue), 1 bottom-up (bitmap)
+    int32_t fcount;       // vertices in the current frontier
+    int32_t ncount;       // vertices reached this level (next frontier)
+    long long nedges;     // out-edges of the next frontier
+    long long uedges;     // out-edges of the vertices not reached yet
+    int32_t cur;          // which queue is the current one
+    int32_t bcur;         // which of the three bitmaps is the current one
+    int32_t alpha, beta;  // top-down -> bottom-up when frontier edges > unvisited edges / alpha;
+                          // back when frontier vertices < n / beta
+    int32_t max_level;
+    int32_t direction;    // 0 switch by the rule above, 1 top-down only, 2 bottom-up only
+    int32_t nchunks;      // heavy-row chunks appended this level
+};
+
+struct Bfs1Bufs {
+    const int32_t* rp;   // CSR
+    const int32_t* col;
+    const int32_t* crp;  // CSC (in-edges)
+    const int32_t* crow;
+    int64_t n;
+    int32_t* lv;
+    int32_t* q[2];
+    uint32_t* bm[3];
+    int64_t nwords;
+    Chunk* chunks;
+};
+
+// Per level: the queue and bitmap of the next frontier and the out-edges of
+// the vertices recorded in them.
+struct BfsNext {
+    using V = int32_t;
+    const int32_t* rp;
+    const int32_t* col;
+    int32_t* lv;
+    int32_t next;  // the level being assigned
+    int32_t* qn;
+    uint32_t* bn;
+    int32_t* ncount;
+    long long edges;
+
+    __device__ V load(int32_t) const { return 0; }
+    __device__ __forceinline__ void record(bool found, int32_t v) {
+        queue_append(found, v, qn, ncount);
+        if (found) {
+            atomicOr(bn + (v >> 5), 1u << (v & 31));
+            edges += rp[v + 1] - rp[v];
+        }
+    }
+    // top-down: claim an unvisited column
+    __device__ __forceinline__ void edge(bool valid, V, int32_t e) {
+        int32_t v = -1;
+        bool found = false;
+        if (valid) {
+            v = col[e];
+            found = lv[v] == 0 && atomicCAS(lv + v, 0, next) == 0;
+        }
+        record(found, v);
+    }
+    __device__ void flush(long long* total) {
+        for (int o = 16; o; o >>= 1) edges += __shfl_xor_sync(kAll, edges, o);
+        if ((threadIdx.x & 31) == 0 && edges) atomicAdd((unsigned long long*)total, (unsigned long long)edges);
+    }
+};
+
+__device__ __forceinline__ BfsNext bfs_next(const Bfs1Bufs& b, Bfs1State* st) {
+    return BfsNext{b.rp, b.col, b.lv, st->level + 1, b.q[st->cur ^ 1], b.bm[(st->bcur + 1) % 3], &st->ncount, 0};
+}
+
+// Top-down rows under kHeavy entries (and the chunks of longer ones), or the
+// whole bottom-up level.
+__global__ void __launch_bounds__(kT) k_bfs1_light(Bfs1Bufs b, Bfs1State* st) {
+    BfsNext op = bfs_next(b, st);
+    const uint32_t* bc = b.bm[st->bcur];
+    uint32_t* bz = b.bm[(st->bcur + 2) % 3];  // the bitmap after next, cleared now
+    const int64_t tid = (int64_t)blockIdx.x * kT + threadIdx.x, nth = (int64_t)gridDim.x * kT;
+    for (int64_t i = tid; i < b.nwords; i += nth) bz[i] = 0;
+    if (st->mode == 0) {
+        expand_light(b.q[st->cur], st->fcount, b.rp, b.chunks, &st->nchunks, op);
+    } else {
+        // every unvisited vertex looks for an in-neighbour in the frontier:
+        // rows under kHeavy entries by their lane, longer ones by the whole
+        // warp 32 entries at a time
+        const int lane = threadIdx.x & 31;
+        const int64_t nr = (b.n + 31) / 32 * 32;
+        for (int64_t v0 = tid; v0 < nr; v0 += nth) {
+            const int32_t v = (int32_t)v0;
+            const bool un = v0 < b.n && b.lv[v] == 0;
+            const int32_t beg = un ? b.crp[v] : 0, deg = un ? b.crp[v + 1] - beg : 0;
+            bool found = false;
+            if (deg < kHeavy)
+                for (int32_t e = beg; e < beg + deg; ++e) {
+                    const int32_t u = b.crow[e];
+                    if ((bc[u >> 5] >> (u & 31)) & 1u) {
+                        found = true;
+                        break;
+                    }
+                }
+            unsigned hubs = __ballot_sync(kAll, deg >= kHeavy);
+            while (hubs) {
+                const int h = __ffs(hubs) - 1;
+                hubs &= hubs - 1;
+                const int32_t hb = __shfl_sync(kAll, beg, h), hd = __shfl_sync(kAll, deg, h);
+                bool hf = false;
+                for (int32_t e0 = 0; e0 < hd && !hf; e0 += 32) {
+                    bool f = false;
+                    if (e0 + lane < hd) {
+                        const int32_t u = b.crow[hb + e0 + lane];
+                        f = (bc[u >> 5] >> (u & 31)) & 1u;
+                    }
+                    hf = __any_sync(kAll, f);
+                }
+                if (lane == h) found = hf;
+            }
+            if (found) b.lv[v] = op.next;
+            op.record(found, v);
+        }
+    }
+    op.flush(&st->nedges);
+}
+
+__global__ void __launch_bounds__(kT) k_bfs1_heavy(Bfs1Bufs b, Bfs1State* st) {
+    if (st->mode != 0) return;
+    BfsNext op = bfs_next(b, st);
+    expand_heavy(b.chunks, st->nchunks, b.rp, op);
+    op.flush(&st->nedges);
+}
+
+__global__ void k_bfs1_control(Bfs1State* st, int64_t n, cudaGraphConditionalHandle h) {
+    if (threadIdx.x != 0) return;
+    const int32_t nc = st->ncount;
+    const long long ne = st->nedges;
+    st->uedges -= ne;
+    const bool cont = nc > 0 && st->level < st->max_level;
+    if (cont && st->direction == 0) {
+        if (st->mode == 0) {
+            if (ne > st->uedges / st->alpha) st->mode = 1;
+        } else if ((long long)nc * st->beta < n) {
+            st->mode = 0;
+        }
+    }
+    if (cont) {
+        st->fcount = nc;
+        st->level += 1;
+        st->cur ^= 1;
+        st->bcur = (st->bcur + 1) % 3;
+    }
+    st->ncount = 0;
+    st->nedges = 0;
+    st->nchunks = 0;
+    cudaGraphSetConditional(h, cont ? 1u : 0u);
+}
+
+__global__ void k_bfs1_init(Bfs1Bufs b, Bfs1State* st, int32_t src, long long nnz, int alpha, int beta,
+                            int direction) {
+    const int64_t tid = (int64_t)blockIdx.x * kT + threadIdx.x, nth = (int64_t)gridDim.x * kT;
+    for (int64_t i = tid; i < b.n; i += nth) b.lv[i] = i == src ? 1 : 0;
+    for (int64_t i = tid; i < b.nwords; i += nth) {
+        b.bm[0][i] = (i == (src >> 5)) ? (1u << (src & 31)) : 0u;
+        b.bm[1][i] = 0;
+        b.bm[2][i] = 0;
+    }
+    if (tid == 0) {
+        b.q[0][0] = src;
+        st->level = 1;
+        st->direction = direction;
+        st->mode = direction == 2 ? 1 : 0;
+        st->fcount = 1;
+        st->ncount = 0;
+        st->nedges = 0;
+        st->uedges = nnz - (b.rp[src + 1] - b.rp[src]);
+        st->cur = 0;
+        st->bcur = 0;
+        st->alpha = alpha;
+        st->beta = beta;
+        st->max_level = b.n + 1 < (int64_t)INT32_MAX ? (int32_t)(b.n + 1) : INT32_MAX - 1;
+        st->nchunks = 0;
+    }
+}
+
+template <typename T>
+__global__ void k_levels_out(const int32_t* __restrict__ lv, int64_t n, T* __restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x;
+    if (i < n) out[i] = (T)lv[i];
+}
+
+// ---- SSSP -------------------------------------------------------------------
+
+struct Sssp1State {
+    int32_t round;
+    int32_t cur;
+    int32_t fcount;
+    int32_t ncount;
+    int32_t max_rounds;
+    int32_t nchunks;
+};
+
+template <typename T>
+struct Sssp1Bufs {
+    const int32_t* rp;
+    const int32_t* col;
+    const T* w;
+    int64_t n;
+    T* dist;
+    int32_t* q[2];
+    uint32_t* bm[2];
+    int64_t nwords;
+    Chunk* chunks;
+};
+
+// dist[v] = min(dist[v], d); true when d was smaller than the old value
+__device__ __forceinline__ bool atomic_min_improves(float* p, float d) {
+    // order-preserving on the bit patterns: non-negative floats order as
+    // ints, negative ones in reverse as unsigned ints
+    if (d >= 0.0f) return __int_as_float(atomicMin((int*)p, __float_as_int(d))) > d;
+    return __uint_as_float(atomicMax((unsigned*)p, __float_as_uint(d))) > d;
+}
+__device__ __forceinline__ bool atomic_min_improves(int32_t* p, int32_t d) { return atomicMin(p, d) > d; }
+
+template <typename T>
+struct SsspRelax {
+    using V = T;
+    const int32_t* col;
+    const T* w;
+    T* dist;
+    int32_t* qn;
+    uint32_t* bn;
+    int32_t* ncount;
+
+    __device__ V load(int32_t u) const { return __ldcg(dist + u); }
+    __device__ __forceinline__ void edge(bool valid, V du, int32_t e) {
+        int32_t v = -1;
+        bool found = false;
+        if (valid) {
+            v = col[e];
+            const T nd = elem_add(du, w[e]);
+            if (nd < __ldcg(dist + v) && atomic_min_improves(dist + v, nd)) {
+                const uint32_t bit = 1u << (v & 31);
+                found = !(atomicOr(bn + (v >> 5), bit) & bit);  // queued once per round
+            }
+        }
+        queue_append(found, v, qn, ncount);
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ SsspRelax<T> sssp_relax(const Sssp1Bufs<T>& b, Sssp1State* st) {
+    return SsspRelax<T>{b.col, b.w, b.dist, b.q[st->cur ^ 1], b.bm[st->round & 1], &st->ncount};
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kT) k_sssp1_light(Sssp1Bufs<T> b, Sssp1State* st) {
+    SsspRelax<T> op = sssp_relax(b, st);
+    uint32_t* bz = b.bm[(st->round + 1) & 1];  // next round's bitmap, cleared now
+    const int64_t tid = (int64_t)blockIdx.x * kT + threadIdx.x, nth = (int64_t)gridDim.x * kT;
+    for (int64_t i = tid; i < b.nwords; i += nth) bz[i] = 0;
+    expand_light(b.q[st->cur], st->fcount, b.rp, b.chunks, &st->nchunks, op);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kT) k_sssp1_heavy(Sssp1Bufs<T> b, Sssp1State* st) {
+    SsspRelax<T> op = sssp_relax(b, st);
+    expand_heavy(b.chunks, st->nchunks, b.rp, op);
+}
+
+__global__ void k_sssp1_control(Sssp1State* st, cudaGraphConditionalHandle h) {
+    if (threadIdx.x != 0) return;
+    const int32_t nc = st->ncount;
+    const bool cont = nc > 0 && st->round < st->max_rounds;
+    if (cont) {
+        st->fcount = nc;
+        st->cur ^= 1;
+        st->round += 1;
+    }
+    st->ncount = 0;
+    st->nchunks = 0;
+    cudaGraphSetConditional(h, cont ? 1u : 0u);
+}
+
+template <typename T>
+__global__ void k_sssp1_init(Sssp1Bufs<T> b, Sssp1State* st, int32_t src) {
+    const int64_t tid = (int64_t)blockIdx.x * kT + threadIdx.x, nth = (int64_t)gridDim.x * kT;
+    for (int64_t i = tid; i < b.n; i += nth) b.dist[i] = i == src ? T(0) : Lim<T>::max();
+    for (int64_t i = tid; i < b.nwords; i += nth) {
+        b.bm[0][i] = 0;
+        b.bm[1][i] = 0;
+    }
+    if (tid == 0) {
+        b.q[0][0] = src;
+        st->round = 1;
+        st->cur = 0;
+        st->fcount = 1;
+        st->ncount = 0;
+        st->max_rounds = b.n < (int64_t)INT32_MAX ? (int32_t)b.n : INT32_MAX;
+        st->nchunks = 0;
+    }
+}
+
+template <typename T>
+int run_sssp1(gbk_matrix A, int32_t source, T* dist, int32_t* rounds, cudaStream_t s) {
+    const int64_t n = A->csr.nrows;
+    Sssp1Bufs<T> b{};
+    b.rp = A->csr.ptr;
+    b.col = A->csr.idx;
+    b.w = (const T*)A->csr.val;
+    b.n = n;
+    b.nwords = (n + 31) / 32;
+    b.dist = dist;
+    void* mem = nullptr;
+    const size_t st_b = 256, q_b = 4 * (size_t)n, bm_b = 4 * (size_t)b.nwords,
+                 ch_b = sizeof(Chunk) * (size_t)max_chunks(A->csr.nnz);
+    GBK_CUDA(cudaMallocAsync(&mem, st_b + ch_b + 2 * q_b + 2 * bm_b, s));
+    char* m = (char*)mem;
+    Sssp1State* st = (Sssp1State*)m;
+    b.chunks = (Chunk*)(m + st_b);
+    m += st_b + ch_b;
+    b.q[0] = (int32_t*)m;
+    b.q[1] = (int32_t*)(m + q_b);
+    b.bm[0] = (uint32_t*)(m + 2 * q_b);
+    b.bm[1] = (uint32_t*)(m + 2 * q_b + bm_b);
+    const int grid = blocks_for_sm((const void*)k_sssp1_light<T>);
+    k_sssp1_init<T><<<grid, kT, 0, s>>>(b, st, source);
+    cudaError_t e = cudaGetLastError();
+    int rc = e == cudaSuccess ? GBK_SUCCESS : cuda_fail(e, "k_sssp1_init", __FILE__, __LINE__);
+    count_launch(1);
+    if (rc == GBK_SUCCESS)
+        rc = run_loop_graph(s, [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
+            k_sssp1_light<T><<<grid, kT, 0, cs>>>(b, st);
+            k_sssp1_heavy<T><<<grid, kT, 0, cs>>>(b, st);
+            k_sssp1_control<<<1, 32, 0, cs>>>(st, h);
+        });
+    if (rc == GBK_SUCCESS && rounds) {
+        Sssp1State h{};
+        e = cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = cuda_fail(e, "SSSP rounds", __FILE__, __LINE__);
+        *rounds = h.round;
+    }
+    cudaFreeAsync(mem, s);
+    return rc;
+}
+
+// ---- CC ---------------------------------------------------------------------
+
+__device__ __forceinline__ int32_t uf_find(int32_t* p, int32_t x) {
+    // path halving; a vertex only ever moves to a smaller root
+    int32_t px = __ldcg(p + x);
+    while (px != x) {
+        const int32_t ppx = __ldcg(p + px);
+        if (ppx != px) p[x] = ppx;
+        x = px;
+        px = ppx;
+    }
+    return x;
+}
+
+__device__ __forceinline__ void uf_unite(int32_t* p, int32_t a, int32_t b) {
+    for (;;) {
+        a = uf_find(p, a);
+        b = uf_find(p, b);
+        if (a == b) return;
+        if (a < b) {
+            const int32_t t = a;
+            a = b;
+            b = t;
+        }
+        // link the larger root a under the smaller root b
+        if (atomicCAS(p + a, a, b) == a) return;
+    }
+}
+
+__global__ void k_cc_init(int32_t* p, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x;
+    if (i < n) p[i] = (int32_t)i;
+}
+
+// Every vertex links along its entry r (r = 0, 1).
+__global__ void k_cc_link_entry(const int32_t* __restrict__ rp, const int32_t* __restrict__ col, int64_t n,
+                                int32_t* p, int r) {
+    const int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x;
+    if (i >= n) return;
+    const int32_t u = (int32_t)i, beg = rp[u];
+    if (rp[u + 1] - beg > r) {
+        const int32_t v = col[beg + r];
+        if (v != u) uf_unite(p, u, v);
+    }
+}
+
+__global__ void k_cc_compress(int32_t* p, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x;
+    if (i < n) p[i] = uf_find(p, (int32_t)i);
+}
+
+// The most frequent root among 1024 sampled vertices (ties: the smaller
+// root), one block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_cc_sample_mode(int32_t* p, int64_t n, int32_t* mode) {
+    __shared__ int32_t roots[1024];
+    __shared__ unsigned long long best;
+    const int i = threadIdx.x;
+    const uint64_t h = (uint64_t)(i + 1) * 0x9E3779B97F4A7C15ull;
+    roots[i] = uf_find(p, (int32_t)((h >> 20) % (uint64_t)n));
+    if (i == 0) best = 0;
+    __syncthreads();
+    const int32_t mine = roots[i];
+    uint32_t count = 0;
+    for (int k = 0; k < 1024; ++k) count += roots[k] == mine;
+    atomicMax(&best, ((unsigned long long)count << 32) | (uint32_t)(INT32_MAX - mine));
+    __syncthreads();
+    if (i == 0) *mode = INT32_MAX - (int32_t)(uint32_t)(best & 0xffffffffu);
+}
+
+// Vertices outside the sampled component (every vertex when skip == 0) link
+// along their entries from the third on: rows under kHeavy entries by their
+// lane, longer ones by the whole warp.
+__global__ void __launch_bounds__(kT) k_cc_link_rest(const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+                                                     int64_t n, int32_t* p, const int32_t* mode, int skip) {
+    const int lane = threadIdx.x & 31;
+    const int32_t c = skip ? *mode : -1;
+    const int64_t tid = (int64_t)blockIdx.x * kT + threadIdx.x, nth = (int64_t)gridDim.x * kT;
+    const int64_t nr = (n + 31) / 32 * 32;
+    for (int64_t u0 = tid; u0 < nr; u0 += nth) {
+        const int32_t u = (int32_t)u0;
+        // after the compression every member of the sampled component points at its root
+        const bool act = u0 < n && __ldcg(p + u) != c;
+        const int32_t beg = act ? rp[u] + 2 : 0, deg = act ? max(rp[u + 1] - beg, 0) : 0;
+        if (deg < kHeavy)
+            for (int32_t e = beg; e < beg + deg; ++e) {
+                const int32_t v = col[e];
+                if (v != u) uf_unite(p, u, v);
+            }
+        unsigned hubs = __ballot_sync(kAll, deg >= kHeavy);
+        while (hubs) {
+            const int h = __ffs(hubs) - 1;
+            hubs &= hubs - 1;
+            const int32_t hu = __shfl_sync(kAll, u, h), hb = __shfl_sync(kAll, beg, h),
+                          hd = __shfl_sync(kAll, deg, h);
+            for (int32_t e = lane; e < hd; e += 32) {
+                const int32_t v = col[hb + e];
+                if (v != hu) uf_unite(p, hu, v);
+            }
+        }
+    }
+}
+
+template <typename T>
+__global__ void k_cc_labels(int32_t* p, int64_t n, T* __restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x;
+    if (i < n) out[i] = (T)uf_find(p, (int32_t)i);
+}
+
+// The CSC lists every column's rows in ascending order; the pattern is
+// symmetric exactly when it equals the CSR, whose rows are then sorted too.
+__global__ void k_same_pattern(const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+                               const int32_t* __restrict__ cp, const int32_t* __restrict__ row, int64_t n,
+                               int64_t nnz, int32_t* diff) {
+    const int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x;
+    bool d = (i <= n && rp[i] != cp[i]) || (i < nnz && col[i] != row[i]);
+    if (__any_sync(kAll, d) && (threadIdx.x & 31) == 0) atomicOr(diff, 1);
+}
+
+int pattern_symmetric(gbk_matrix A, cudaStream_t s, bool* out) {
+    if (A->pattern_symmetric < 0) {
+        const int64_t n = A->csr.nrows;
+        if (A->csr.ncols != n) {
+            A->pattern_symmetric = 0;
+        } else {
+            int rc = ensure_csc(A, s);
+            if (rc) return rc;
+            int32_t* diff = nullptr;
+            GBK_CUDA(cudaMallocAsync((void**)&diff, 4, s));
+            GBK_CUDA(cudaMemsetAsync(diff, 0, 4, s));
+            const int64_t cnt = std::max<int64_t>(n + 1, A->csr.nnz);
+            k_same_pattern<<<grid1(cnt), kT, 0, s>>>(A->csr.ptr, A->csr.idx, A->csc.ptr, A->csc.idx, n,
+                                                      A->csr.nnz, diff);
+            GBK_LAUNCHED();
+            int32_t h = 1;
+            cudaError_t e = cudaMemcpyAsync(&h, diff, 4, cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            cudaFreeAsync(diff, s);
+            if (e != cudaSuccess) return cuda_fail(e, "pattern symmetry check", __FILE__, __LINE__);
+            A->pattern_symmetric = h == 0 ? 1 : 0;
+        }
+    }
+    *out = A->pattern_symmetric == 1;
+    return GBK_SUCCESS;
+}
+
+}  // namespace
+
+}  // namespace gbk
+
+using namespace gbk;
+
+extern "C" int gbk_bfs_levels(gbk_matrix A, int64_t source, int direction, gbk_dtype level_type, void* levels,
+                              int32_t* depth, void* stream) {
+    GBK_REQUIRE(A && levels, GBK_NULL_POINTER, "gbk_bfs_levels: NULL argument");
+    const int64_t n = A->csr.nrows;
+    GBK_REQUIRE(A->csr.ncols == n, GBK_DIMENSION_MISMATCH, "gbk_bfs_levels: the matrix must be square");
+    GBK_REQUIRE(source >= 0 && source < n, GBK_INVALID_INDEX, "gbk_bfs_levels: source %lld outside [0, %lld)",
+                (long long)source, (long long)n);
+    GBK_REQUIRE(direction >= 0 && direction <= 2, GBK_INVALID_VALUE, "gbk_bfs_levels: direction %d", direction);
+    GBK_REQUIRE(level_type == GBK_F32 || level_type == GBK_I32 || level_type == GBK_F64 || level_type == GBK_I64,
+                GBK_INVALID_VALUE, "gbk_bfs_levels: level type %d", (int)level_type);
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = ensure_csc(A, s);
+    if (rc) return rc;
+    Bfs1Bufs b{};
+    b.rp = A->csr.ptr;
+    b.col = A->csr.idx;
+    b.crp = A->csc.ptr;
+    b.crow = A->csc.idx;
+    b.n = n;
+    b.nwords = (n + 31) / 32;
+    void* mem = nullptr;
+    const size_t st_b = 256, lv_b = 4 * (size_t)n, q_b = 4 * (size_t)n, bm_b = 4 * (size_t)b.nwords,
+                 ch_b = sizeof(Chunk) * (size_t)max_chunks(A->csr.nnz);
+    GBK_CUDA(cudaMallocAsync(&mem, st_b + ch_b + lv_b + 2 * q_b + 3 * bm_b, s));
+    char* m = (char*)mem;
+    Bfs1State* st = (Bfs1State*)m;
+    b.chunks = (Chunk*)(m + st_b);
+    m += st_b + ch_b;
+    // int32 levels are written in place; other types are converted at the end
+    const bool direct = level_type == GBK_I32;
+    b.lv = direct ? (int32_t*)levels : (int32_t*)m;
+    b.q[0] = (int32_t*)(m + lv_b);
+    b.q[1] = (int32_t*)(m + lv_b + q_b);
+    for (int k = 0; k < 3; ++k) b.bm[k] = (uint32_t*)(m + lv_b + 2 * q_b + k * bm_b);
+    const int grid = blocks_for_sm((const void*)k_bfs1_light);
+    k_bfs1_init<<<grid, kT, 0, s>>>(b, st, (int32_t)source, (long long)A->csr.nnz, 14, 24, direction);
+    cudaError_t e = cudaGetLastError();
+    rc = e == cudaSuccess ? GBK_SUCCESS : cuda_fail(e, "k_bfs1_init", __FILE__, __LINE__);
+    count_launch(1);
+    if (rc == GBK_SUCCESS)
+        rc = run_loop_graph(s, [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
+            k_bfs1_light<<<grid, kT, 0, cs>>>(b, st);
+            k_bfs1_heavy<<<grid, kT, 0, cs>>>(b, st);
+            k_bfs1_control<<<1, 32, 0, cs>>>(st, b.n, h);
+        });
+    if (rc == GBK_SUCCESS && !direct) {
+#define LV_OUT(TY) k_levels_out<TY><<<grid1(n), kT, 0, s>>>(b.lv, n, (TY*)levels)
+        switch (level_type) {
+            case GBK_F32: LV_OUT(float); break;
+            case GBK_F64: LV_OUT(double); break;
+            default: LV_OUT(int64_t); break;
+        }
+#undef LV_OUT
+        e = cudaGetLastError();
+        if (e != cudaSuccess) rc = cuda_fail(e, "level conversion", __FILE__, __LINE__);
+        count_launch(1);
+    }
+    if (rc == GBK_SUCCESS && depth) {
+        Bfs1State h{};
+        e = cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = cuda_fail(e, "BFS depth", __FILE__, __LINE__);
+        *depth = h.level;
+    }
+    cudaFreeAsync(mem, s);
+    return rc;
+}
+
+extern "C" int gbk_sssp_dist(gbk_matrix A, int64_t source, void* dist, int32_t* rounds, void* stream) {
+    GBK_REQUIRE(A && dist, GBK_NULL_POINTER, "gbk_sssp_dist: NULL argument");
+    const int64_t n = A->csr.nrows;
+    GBK_REQUIRE(A->csr.ncols == n, GBK_DIMENSION_MISMATCH, "gbk_sssp_dist: the matrix must be square");
+    GBK_REQUIRE(source >= 0 && source < n, GBK_INVALID_INDEX, "gbk_sssp_dist: source %lld outside [0, %lld)",
+                (long long)source, (long long)n);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (A->vtype == GBK_F32) return run_sssp1<float>(A, (int32_t)source, (float*)dist, rounds, s);
+    return run_sssp1<int32_t>(A, (int32_t)source, (int32_t*)dist, rounds, s);
+}
+
+extern "C" int gbk_matrix_pattern_symmetric(gbk_matrix A, int32_t* symmetric, void* stream) {
+    GBK_REQUIRE(A && symmetric, GBK_NULL_POINTER, "gbk_matrix_pattern_symmetric: NULL argument");
+    bool sym = false;
+    int rc = pattern_symmetric(A, (cudaStream_t)stream, &sym);
+    if (rc) return rc;
+    *symmetric = sym ? 1 : 0;
+    return GBK_SUCCESS;
+}
+
+extern "C" int gbk_cc_labels(gbk_matrix A, gbk_dtype label_type, void* labels, void* stream) {
+    GBK_REQUIRE(A && labels, GBK_NULL_POINTER, "gbk_cc_labels: NULL argument");
+    const int64_t n = A->csr.nrows;
+    GBK_REQUIRE(A->csr.ncols == n, GBK_DIMENSION_MISMATCH, "gbk_cc_labels: the matrix must be square");
+    GBK_REQUIRE(label_type == GBK_F32 || label_type == GBK_I32 || label_type == GBK_I64, GBK_INVALID_VALUE,
+                "gbk_cc_labels: label type %d", (int)label_type);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (n == 0) return GBK_SUCCESS;
+    bool sym = false;
+    int rc = pattern_symmetric(A, s, &sym);
+    if (rc) return rc;
+    // int32 labels: the forest lives in the output itself
+    const bool direct = label_type == GBK_I32;
+    int32_t* p = (int32_t*)labels;
+    int32_t* mode = nullptr;
+    GBK_CUDA(cudaMallocAsync((void**)&mode, direct ? 16 : 16 + 4 * (size_t)n, s));
+    if (!direct) p = mode + 4;
+    const unsigned g = grid1(n);
+    k_cc_init<<<g, kT, 0, s>>>(p, n);
+    GBK_LAUNCHED();
+    for (int r = 0; r < 2; ++r) {
+        k_cc_link_entry<<<g, kT, 0, s>>>(A->csr.ptr, A->csr.idx, n, p, r);
+        GBK_LAUNCHED();
+        k_cc_compress<<<g, kT, 0, s>>>(p, n);
+        GBK_LAUNCHED();
+    }
+    k_cc_sample_mode<<<1, 1024, 0, s>>>(p, n, mode);
+    GBK_LAUNCHED();
+    k_cc_link_rest<<<blocks_for_sm((const void*)k_cc_link_rest), kT, 0, s>>>(A->csr.ptr, A->csr.idx, n, p, mode,
+                                                                              sym ? 1 : 0);
+    GBK_LAUNCHED();
+    switch (label_type) {
+        case GBK_F32: k_cc_labels<float><<<g, kT, 0, s>>>(p, n, (float*)labels); break;
+        case GBK_I32: k_cc_compress<<<g, kT, 0, s>>>(p, n); break;
+        default: k_cc_labels<int64_t><<<g, kT, 0, s>>>(p, n, (int64_t*)labels); break;
+    }
+    GBK_LAUNCHED();
+    cudaFreeAsync(mode, s);
+    return GBK_SUCCESS;
+}

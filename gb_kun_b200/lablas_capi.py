@@ -34,7 +34,10 @@ def lib():
         L.gbk_lablas_get_last_error.argtypes = [C.c_char_p, C.c_size_t]
         L.gbk_lablas_bfs.argtypes = [vp, i64, vp, dp]
         L.gbk_lablas_cc.argtypes = [vp, vp, C.POINTER(i32), dp]
+        L.gbk_lablas_bfs_ops.argtypes = [vp, i64, vp, dp]
+        L.gbk_lablas_cc_fastsv.argtypes = [vp, vp, C.POINTER(i32), dp]
         L.gbk_lablas_sssp_f32.argtypes = [vp, i64, vp, dp]
+        L.gbk_lablas_sssp_f32_ops.argtypes = [vp, i64, vp, dp]
         L.gbk_lablas_sssp_i32.argtypes = [vp, i64, vp, dp]
         L.gbk_lablas_pagerank.argtypes = [vp, i32, C.c_double, C.c_double, vp, C.POINTER(i32), dp]
         L.gbk_lablas_ppr.argtypes = [vp, i64, i32, C.c_double, C.c_double, vp, C.POINTER(i32), dp]
@@ -99,6 +102,13 @@ class Graph:
         _check(lib().gbk_lablas_bfs(self.h, int(source), _p(out), C.byref(ms)), "bfs")
         return out, ms.value
 
+    def bfs_ops(self, source):
+        """bfs_blast as its sequence of GraphBLAS calls (one host read per level)."""
+        out = np.empty(self.n, np.int32)
+        ms = C.c_double()
+        _check(lib().gbk_lablas_bfs_ops(self.h, int(source), _p(out), C.byref(ms)), "bfs_ops")
+        return out, ms.value
+
     def cc(self):
         out = np.empty(self.n, np.int32)
         it = C.c_int32()
@@ -106,10 +116,25 @@ class Graph:
         _check(lib().gbk_lablas_cc(self.h, _p(out), C.byref(it), C.byref(ms)), "cc")
         return out, ms.value
 
+    def cc_fastsv(self):
+        """The FastSV loop as the reference writes it; returns (labels, iterations, ms)."""
+        out = np.empty(self.n, np.int32)
+        it = C.c_int32()
+        ms = C.c_double()
+        _check(lib().gbk_lablas_cc_fastsv(self.h, _p(out), C.byref(it), C.byref(ms)), "cc_fastsv")
+        return out, it.value, ms.value
+
     def sssp_f32(self, source):
         out = np.empty(self.n, np.float32)
         ms = C.c_double()
         _check(lib().gbk_lablas_sssp_f32(self.h, int(source), _p(out), C.byref(ms)), "sssp_f32")
+        return out, ms.value
+
+    def sssp_f32_ops(self, source):
+        """sssp_bellman_ford_blast as its sequence of GraphBLAS calls (a host read per round)."""
+        out = np.empty(self.n, np.float32)
+        ms = C.c_double()
+        _check(lib().gbk_lablas_sssp_f32_ops(self.h, int(source), _p(out), C.byref(ms)), "sssp_f32_ops")
         return out, ms.value
 
     def sssp_i32(self, source):

@@ -260,6 +260,50 @@ int gbk_ppr(gbk_matrix A, const int32_t* seeds, int nseeds, double damping, doub
  * Synchronises the stream. */
 int gbk_sssp_multi(gbk_matrix A, const int32_t* sources, int nsources, int32_t* dist, int32_t* iters, void* stream);
 
+/* ---- single-query traversals (the whole loop on the device) ------------- */
+
+/* Single-source BFS with the result of bfs_blast (algorithms/bfs/bfs.hpp:94-142,
+ * edges followed along the rows of A): levels[v] = 1 for the source, k + 1 at
+ * distance k, 0 unreached.  levels is device memory of n elements of
+ * level_type (GBK_F32 as the reference's Vector<float>, GBK_I32, GBK_I64,
+ * GBK_F64).  Direction-optimising: each level expands top-down from a queue
+ * or bottom-up over the unvisited vertices' in-edges (the CSC, built on first
+ * use) as the frontier's edge count decides (direction 0; 1 top-down only,
+ * 2 bottom-up only, same levels); the level loop runs as one CUDA graph with
+ * a device-side `while` node, so the call issues one graph launch whatever
+ * the depth.  depth (host, may be NULL) receives the largest level and then
+ * the call synchronises the stream; with depth NULL it does not. */
+int gbk_bfs_levels(gbk_matrix A, int64_t source, int direction, gbk_dtype level_type, void* levels, int32_t* depth,
+                   void* stream);
+/* Single-source shortest paths with the distances of sssp_bellman_ford_blast
+ * (algorithms/sssp/sssp_blast.hpp:8-72): dist[v] = the smallest sum of edge
+ * values (the matrix values) over the walks from source to v, added left to
+ * right in the matrix's value type (GBK_F32: float, FLT_MAX = unreachable;
+ * GBK_I32: saturating int32, INT32_MAX = unreachable); dist[source] = 0.
+ * dist is device memory of n elements of the matrix's value type.  A
+ * label-correcting worklist: each round relaxes the out-edges (rows of A) of
+ * the vertices whose distance dropped in the round before; all rounds run as
+ * one CUDA graph with a device-side `while` node.  Negative edge values are
+ * allowed; with a negative cycle reachable the rounds stop after n and the
+ * distances are not defined (the reference's n-round bound gives other
+ * values there).  rounds (host, may be NULL) receives the rounds run and then
+ * the call synchronises the stream; with rounds NULL it does not. */
+int gbk_sssp_dist(gbk_matrix A, int64_t source, void* dist, int32_t* rounds, void* stream);
+/* *symmetric = 1 when A is square and its pattern equals its transpose's with
+ * every row's column indices ascending, else 0 (an unsorted symmetric matrix
+ * reads as 0).  Computed once per matrix on the device against its CSC. */
+int gbk_matrix_pattern_symmetric(gbk_matrix A, int32_t* symmetric, void* stream);
+/* Connected components as the label of each vertex = the smallest vertex id
+ * of its component: the fixed point of the FastSV loop in cc
+ * (algorithms/cc/cc.hpp:12-119) on a symmetric A.  Lock-free union-find over
+ * the stored edges, each linking the larger root under the smaller, then one
+ * pass taking every vertex's root: three kernel launches, no host round
+ * trip.  Edges count in both directions, so a non-symmetric A gets its weakly
+ * connected components (FastSV's answer can differ there; callers that must
+ * reproduce it check gbk_matrix_pattern_symmetric first).  labels is device
+ * memory of n elements of label_type (GBK_I32, GBK_I64 or GBK_F32). */
+int gbk_cc_labels(gbk_matrix A, gbk_dtype label_type, void* labels, void* stream);
+
 /* Tuning of the batched traversals on this graph: times each candidate on
  * the given sources (CUDA events, best of 2 after a warm-up) and keeps the
  * fastest for later gbk_msbfs / gbk_ppr / gbk_sssp_multi calls and servers

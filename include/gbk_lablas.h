@@ -32,13 +32,26 @@ int gbk_lablas_graph_from_file(gbk_lablas_graph* out, const char* path);
 int gbk_lablas_graph_destroy(gbk_lablas_graph g);
 int gbk_lablas_get_last_error(char* buf, size_t len);
 
-/* bfs_blast (algorithms/bfs/bfs.hpp:93-142): levels, source = 1, unvisited = 0. */
+/* bfs_blast (algorithms/bfs/bfs.hpp:94-142): levels, source = 1, unvisited = 0,
+ * with the level loop on the device (gbk_bfs_levels). */
 int gbk_lablas_bfs(gbk_lablas_graph g, int64_t source, int32_t* levels, double* ms);
-/* FastSV cc (algorithms/cc/cc.hpp:12-119): component labels. */
+/* The same levels through bfs_blast's own sequence of GraphBLAS calls
+ * (assign, masked vxm, reduce with a host read per level). */
+int gbk_lablas_bfs_ops(gbk_lablas_graph g, int64_t source, int32_t* levels, double* ms);
+/* cc (algorithms/cc/cc.hpp:12-119): component labels = smallest vertex id of
+ * each component; union-find on the device for a symmetric matrix
+ * (*iterations = 0), the FastSV loop otherwise. */
 int gbk_lablas_cc(gbk_lablas_graph g, int32_t* labels, int32_t* iterations, double* ms);
+/* The FastSV loop as cc.hpp writes it, whatever the matrix
+ * (*iterations = its iteration count). */
+int gbk_lablas_cc_fastsv(gbk_lablas_graph g, int32_t* labels, int32_t* iterations, double* ms);
 /* sssp_bellman_ford_blast (algorithms/sssp/sssp_blast.hpp:8-72) in float
  * (weights as exact floats; unreachable = FLT_MAX). */
 int gbk_lablas_sssp_f32(gbk_lablas_graph g, int64_t source, float* dist, double* ms);
+/* The same distances through sssp_bellman_ford_blast's own sequence of
+ * GraphBLAS calls (vxm, eWiseAdds, masked assign, reduce with a host read per
+ * round). */
+int gbk_lablas_sssp_f32_ops(gbk_lablas_graph g, int64_t source, float* dist, double* ms);
 /* The same rounds in int32 (unreachable = INT32_MAX). */
 int gbk_lablas_sssp_i32(gbk_lablas_graph g, int64_t source, int32_t* dist, double* ms);
 /* LAGraph page_rank_sinks (algorithms/pr/pr.hpp:20-153); stops after

@@ -1,0 +1,347 @@
+"""Single-query traversals with the loop on the device (gbk_bfs_levels,
+gbk_cc_labels, gbk_matrix_pattern_symmetric) against the oracle and the
+reference's golden outputs.
+
+* BFS levels equal bfs_blast's (algorithms/bfs/bfs.hpp:94-142) bit-exact in
+  every level type and every direction mode, on directed and undirected
+  graphs, from isolated and hub sources, on a long chain (thousands of
+  levels in one graph launch) and through the lablas:: algorithm both as the
+  fused call and as the reference's own GraphBLAS call sequence.
+* CC labels equal the FastSV fixed point (algorithms/cc/cc.hpp:12-119) on
+  symmetric graphs; a directed graph is reported non-symmetric and the
+  lablas:: cc then runs FastSV itself; gbk_cc_labels on it gives the weakly
+  connected components.
+* SSSP distances equal sssp_bellman_ford_blast's
+  (algorithms/sssp/sssp_blast.hpp:8-72): the reference's golden outputs,
+  integer weights against the oracle, non-integer float weights against a
+  float32 Dijkstra, negative weights on a DAG, and the lablas:: call against
+  the reference's own GraphBLAS call sequence.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_graph
+from gb_kun_b200 import graphgen as gg
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    from gb_kun_b200 import capi
+    capi.init(0)
+    return t
+
+
+def _mat(g):
+    from gb_kun_b200 import capi
+    return capi.Matrix.from_graph(g, np.ones(g.nnz, np.float32))
+
+
+def _levels(torch, A, n, src, dtype=None, direction=0):
+    lv = torch.full((n,), 7, dtype=dtype or torch.int32, device="cuda")
+    depth = A.bfs(int(src), lv, direction=direction)
+    return lv.cpu().numpy(), depth
+
+
+@pytest.mark.parametrize("name", ["rmat10", "rmat11u", "er11u"])
+def test_bfs_golden_every_direction(torch, golden, name):
+    data, _ = golden
+    g = golden_graph(data, name)
+    A = _mat(g)
+    srcs = data[f"{name}.sources"]
+    for k in range(len(srcs)):
+        key = f"{name}.bfs.{k}"
+        if key not in data:
+            continue
+        want = data[key]
+        for d in (0, 1, 2):
+            got, depth = _levels(torch, A, g.n, srcs[k], direction=d)
+            assert np.array_equal(got, want), (name, k, d)
+            assert depth == int(want.max())
+    A.close()
+
+
+@pytest.mark.parametrize("dt", ["float32", "int64", "float64"])
+def test_bfs_level_types(torch, oracle, dt):
+    g = gg.rmat(14, 16, seed=5)
+    A = _mat(g)
+    src = int(gg.sources(g, 1, seed=6)[0])
+    got, _ = _levels(torch, A, g.n, src, dtype=getattr(torch, dt))
+    assert got.dtype == np.dtype(dt)
+    assert np.array_equal(got, oracle.bfs(g, src).astype(dt))
+    A.close()
+
+
+@pytest.mark.parametrize("kind", ["rmat_directed", "rmat_undirected", "uniform_dense"])
+def test_bfs_vs_oracle_many_sources(torch, oracle, kind):
+    if kind == "rmat_directed":
+        g = gg.rmat(16, 16, seed=11)
+    elif kind == "rmat_undirected":
+        g = gg.rmat(16, 16, seed=12, undirected=True)
+    else:
+        g = gg.uniform(14, 64, seed=13)  # dense frontiers: bottom-up levels
+    A = _mat(g)
+    deg = np.diff(g.row_ptr)
+    hub = int(np.argmax(deg))
+    isolated = np.nonzero(deg == 0)[0]
+    srcs = [int(s) for s in gg.sources(g, 4, seed=14)] + [hub, 0, g.n - 1]
+    if len(isolated):
+        srcs.append(int(isolated[0]))
+    for s in srcs:
+        want = oracle.bfs(g, s)
+        for d in (0, 1, 2):
+            got, depth = _levels(torch, A, g.n, s, direction=d)
+            assert np.array_equal(got, want), (kind, s, d)
+            assert depth == int(want.max())
+    A.close()
+
+
+def test_bfs_long_chain_one_graph_launch(torch, oracle):
+    from gb_kun_b200 import capi
+    n = 5000
+    src = np.arange(n - 1)
+    g = gg.from_edges(n, src, src + 1)  # 0 -> 1 -> ... -> n-1
+    A = _mat(g)
+    lv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    A.bfs(0, lv)  # first call builds the CSC
+    before = capi.launch_count()
+    depth = A.bfs(0, lv)
+    launches = capi.launch_count() - before
+    assert depth == n
+    assert np.array_equal(lv.cpu().numpy(), np.arange(1, n + 1, dtype=np.int32))
+    # init + one graph (two kernels per level inside it), whatever the depth
+    assert launches <= 4, launches
+    got, _ = _levels(torch, A, n, n // 2)
+    assert np.array_equal(got, oracle.bfs(g, n // 2))
+    A.close()
+
+
+def test_bfs_self_loops_and_tiny(torch, oracle):
+    g = gg.from_edges(4, [0, 0, 1, 2, 3], [0, 1, 1, 3, 3])
+    A = _mat(g)
+    for s in range(4):
+        got, _ = _levels(torch, A, 4, s)
+        assert np.array_equal(got, oracle.bfs(g, s)), s
+    A.close()
+    g1 = gg.from_edges(1, [], [])
+    A1 = _mat(g1)
+    got, depth = _levels(torch, A1, 1, 0)
+    assert got.tolist() == [1] and depth == 1
+    A1.close()
+
+
+def test_bfs_errors(torch):
+    from gb_kun_b200 import capi
+    g = gg.rmat(8, 4, seed=3)
+    A = _mat(g)
+    lv = torch.zeros(g.n, dtype=torch.int32, device="cuda")
+    with pytest.raises(capi.GbkError):
+        A.bfs(g.n, lv)
+    with pytest.raises(capi.GbkError):
+        A.bfs(-1, lv)
+    with pytest.raises(capi.GbkError):
+        A.bfs(0, lv, direction=3)
+    A.close()
+    B = capi.Matrix(np.array([0, 1, 2], np.int32), np.array([0, 2], np.int32), np.ones(2, np.float32), ncols=3)
+    with pytest.raises(capi.GbkError):
+        B.bfs(0, torch.zeros(2, dtype=torch.int32, device="cuda"))
+    B.close()
+
+
+@pytest.mark.parametrize("name", ["rmat11u", "er11u"])
+def test_cc_golden(torch, golden, name):
+    data, _ = golden
+    g = golden_graph(data, name)
+    A = _mat(g)
+    assert A.pattern_symmetric()
+    for dt in (torch.int32, torch.int64, torch.float32):
+        lab = torch.full((g.n,), -5, dtype=dt, device="cuda")
+        A.cc(lab)
+        assert np.array_equal(lab.cpu().numpy(), data[f"{name}.cc"].astype(lab.cpu().numpy().dtype)), dt
+    A.close()
+
+
+def test_cc_symmetric_vs_oracle(torch, oracle):
+    # many components: a sparse undirected uniform graph plus isolated vertices
+    g = gg.uniform(16, 1, seed=21, undirected=True)
+    A = _mat(g)
+    assert A.pattern_symmetric()
+    lab = torch.zeros(g.n, dtype=torch.int32, device="cuda")
+    A.cc(lab)
+    want = oracle.cc(g)
+    assert len(np.unique(want)) > 1000
+    assert np.array_equal(lab.cpu().numpy(), want)
+    A.close()
+
+
+def _weak_min_labels(g):
+    p = np.arange(g.n)
+
+    def find(x):
+        while p[x] != x:
+            p[x] = p[p[x]]
+            x = p[x]
+        return x
+
+    rows = np.repeat(np.arange(g.n), np.diff(g.row_ptr))
+    for u, v in zip(rows.tolist(), np.asarray(g.col).tolist()):
+        a, b = find(u), find(v)
+        if a != b:
+            p[max(a, b)] = min(a, b)
+    return np.array([find(i) for i in range(g.n)], np.int32)
+
+
+def test_cc_directed_weak_components_and_lablas_fallback(torch):
+    from gb_kun_b200 import lablas_capi as lc
+    g = gg.rmat(12, 4, seed=31)
+    A = _mat(g)
+    assert not A.pattern_symmetric()
+    lab = torch.zeros(g.n, dtype=torch.int32, device="cuda")
+    A.cc(lab)
+    assert np.array_equal(lab.cpu().numpy(), _weak_min_labels(g))
+    A.close()
+    G = lc.Graph(g)
+    fused, _ = G.cc()
+    fastsv, iters, _ = G.cc_fastsv()
+    assert iters > 0
+    assert np.array_equal(fused, fastsv)  # non-symmetric: cc ran FastSV itself
+
+
+def test_lablas_fused_equals_graphblas_sequence(torch, oracle):
+    from gb_kun_b200 import lablas_capi as lc
+    for g in (gg.rmat(15, 16, seed=41, undirected=True), gg.rmat(15, 16, seed=42)):
+        G = lc.Graph(g)
+        for s in gg.sources(g, 3, seed=43):
+            a, _ = G.bfs(int(s))
+            b, _ = G.bfs_ops(int(s))
+            assert np.array_equal(a, b) and np.array_equal(a, oracle.bfs(g, int(s))), int(s)
+    g = gg.rmat(15, 16, seed=44, undirected=True)
+    G = lc.Graph(g)
+    fused, _ = G.cc()
+    fastsv, iters, _ = G.cc_fastsv()
+    assert iters > 0
+    assert np.array_equal(fused, fastsv) and np.array_equal(fused, oracle.cc(g))
+
+
+# ---- SSSP --------------------------------------------------------------------
+
+def _dijkstra(g, w, src, dtype):
+    """Dijkstra with the additions in `dtype` (float32 rounding for float
+    weights; exact int64 sums saturated to INT32_MAX for int weights)."""
+    import heapq
+    inf = np.finfo(np.float32).max if dtype == np.float32 else np.iinfo(np.int32).max
+    d = np.full(g.n, inf, dtype=dtype)
+    d[src] = 0
+    done = np.zeros(g.n, bool)
+    h = [(dtype(0), int(src))]
+    rp, col = g.row_ptr, g.col
+    while h:
+        du, u = heapq.heappop(h)
+        if done[u]:
+            continue
+        done[u] = True
+        for e in range(rp[u], rp[u + 1]):
+            v = int(col[e])
+            nd = dtype(du + w[e]) if dtype == np.float32 else min(int(du) + int(w[e]), inf)
+            if nd < d[v]:
+                d[v] = nd
+                heapq.heappush(h, (nd, v))
+    return d
+
+
+@pytest.mark.parametrize("name", ["rmat11u", "er11u"])
+def test_sssp_golden(torch, golden, name):
+    from gb_kun_b200 import capi
+    data, _ = golden
+    g = golden_graph(data, name)
+    w = data[f"{name}.w"]
+    src = int(data[f"{name}.sources"][0])
+    A = capi.Matrix.from_graph(g, w.astype(np.float32))
+    d = torch.zeros(g.n, dtype=torch.float32, device="cuda")
+    rounds = A.sssp(src, d)
+    assert rounds >= 1
+    assert np.array_equal(d.cpu().numpy(), data[f"{name}.sssp"])
+    A.close()
+
+
+@pytest.mark.parametrize("undirected", [True, False])
+def test_sssp_int_vs_oracle(torch, oracle, undirected):
+    from gb_kun_b200 import capi
+    g = gg.rmat(15, 16, seed=51, undirected=undirected)
+    w = gg.weights_i32(g, seed=52)
+    A = capi.Matrix.from_graph(g, w)
+    d = torch.zeros(g.n, dtype=torch.int32, device="cuda")
+    deg = np.diff(g.row_ptr)
+    for s in [int(x) for x in gg.sources(g, 3, seed=53)] + [int(np.argmax(deg))]:
+        A.sssp(s, d)
+        want = oracle.sssp(g, w, s)
+        assert np.array_equal(d.cpu().numpy(), np.where(want < 0, np.iinfo(np.int32).max, want).astype(np.int32)), s
+    A.close()
+
+
+def test_sssp_float_weights_vs_dijkstra(torch):
+    from gb_kun_b200 import capi
+    g = gg.rmat(11, 8, seed=61)
+    w = (np.random.default_rng(62).random(g.nnz, dtype=np.float32) * 3.7 + 0.01).astype(np.float32)
+    A = capi.Matrix.from_graph(g, w)
+    d = torch.zeros(g.n, dtype=torch.float32, device="cuda")
+    for s in gg.sources(g, 3, seed=63):
+        A.sssp(int(s), d)
+        assert np.array_equal(d.cpu().numpy(), _dijkstra(g, w, int(s), np.float32)), int(s)
+    A.close()
+
+
+def test_sssp_negative_weights_dag(torch):
+    from gb_kun_b200 import capi
+    # a DAG (edges from smaller to larger ids) with some negative weights
+    rng = np.random.default_rng(71)
+    n = 3000
+    src = rng.integers(0, n - 1, 20000)
+    dst = np.minimum(src + 1 + rng.integers(0, 50, 20000), n - 1)
+    g = gg.from_edges(n, src, dst)
+    w = rng.integers(-20, 100, g.nnz).astype(np.int32)
+    A = capi.Matrix.from_graph(g, w)
+    d = torch.zeros(n, dtype=torch.int32, device="cuda")
+    A.sssp(0, d)
+    # Bellman-Ford in topological (id) order is exact on a DAG
+    want = np.full(n, np.iinfo(np.int32).max, np.int64)
+    want[0] = 0
+    for u in range(n):
+        if want[u] == np.iinfo(np.int32).max:
+            continue
+        for e in range(g.row_ptr[u], g.row_ptr[u + 1]):
+            v = g.col[e]
+            want[v] = min(want[v], want[u] + w[e])
+    assert np.array_equal(d.cpu().numpy(), want.astype(np.int32))
+    A.close()
+
+
+def test_sssp_errors_and_single_vertex(torch):
+    from gb_kun_b200 import capi
+    g = gg.rmat(8, 4, seed=3)
+    A = _mat(g)
+    d = torch.zeros(g.n, dtype=torch.float32, device="cuda")
+    with pytest.raises(capi.GbkError):
+        A.sssp(g.n, d)
+    A.close()
+    g1 = gg.from_edges(1, [0], [0])
+    A1 = capi.Matrix.from_graph(g1, np.array([5.0], np.float32))
+    d1 = torch.full((1,), 3.0, device="cuda")
+    A1.sssp(0, d1)
+    assert d1.cpu().numpy().tolist() == [0.0]
+    A1.close()
+
+
+def test_lablas_sssp_fused_equals_graphblas_sequence(torch, oracle):
+    from gb_kun_b200 import lablas_capi as lc
+    g = gg.rmat(15, 16, seed=81, undirected=True)
+    w = gg.weights_i32(g, seed=82)
+    G = lc.Graph(g, weights=w)
+    for s in gg.sources(g, 2, seed=83):
+        a, _ = G.sssp_f32(int(s))
+        b, _ = G.sssp_f32_ops(int(s))
+        d64 = oracle.sssp(g, w, int(s))
+        assert np.array_equal(a, b)
+        assert np.array_equal(a, np.where(d64 < 0, np.finfo(np.float32).max, d64).astype(np.float32))
