@@ -26,6 +26,7 @@ Multi-GPU: the hot path does not need an exchange at these sizes, so
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -238,12 +239,20 @@ def read_traffic(profile):
     """DRAM bytes of one SpMV from the committed ncu summary.
 
     Prefers the whole-SpMV sum (`traffic_bytes_per_spmv:`, all kernels of one
-    SpMV from the launch list), else the dominant kernel's own launch."""
+    SpMV from the launch list), else the dominant kernel's own launch.  The
+    summary names the kernel sources it was captured from
+    (`kernel_source_sha256: <path> <hex>`); when a source has changed since,
+    the figure describes other code and None is returned."""
     f = ROOT / "profiles" / f"{profile}.md"
     if not f.exists():
         return None
     found = {}
     for line in f.read_text().splitlines():
+        if line.startswith("kernel_source_sha256:"):
+            parts = line.split(":", 1)[1].split()
+            src = ROOT / parts[0]
+            if len(parts) < 2 or not src.exists() or hashlib.sha256(src.read_bytes()).hexdigest() != parts[1]:
+                return None
         for key in ("traffic_bytes_per_spmv:", "traffic_bytes_per_launch:"):
             if line.startswith(key) and key not in found:
                 try:

@@ -6,6 +6,12 @@
 // Unlike the reference, which always runs itermax iterations, the loop stops
 // once rdiff < tol when tol > 0 (the stopping rule LAGraph documents); with
 // tol <= 0 it runs exactly itermax iterations like the reference.
+//
+//  * page_rank_sinks runs the loop on the device (gbk_pagerank: the SpMV in
+//    the matrix's format, one fused element-wise pass, a control kernel; one
+//    CUDA graph for the iterations).
+//  * page_rank_sinks_ops is the same iteration as the reference's sequence
+//    of GraphBLAS calls, with a host read of rdiff per iteration.
 #pragma once
 
 #include "lablas/gb_kun.h"
@@ -15,6 +21,14 @@ namespace algorithm {
 
 inline void page_rank_sinks(Vector<float>* centrality, LAGraph_Graph<float>* G, int* iters, int itermax = 100,
                             double damping = 0.85, double tol = 1e-4) {
+    int32_t it = 0;
+    throw_if(gbk_pagerank(G->AT->handle(), itermax, damping, tol, centrality->dense_ptr(), &it, nullptr, stream()),
+             "page_rank_sinks");
+    *iters = it;
+}
+
+inline void page_rank_sinks_ops(Vector<float>* centrality, LAGraph_Graph<float>* G, int* iters, int itermax = 100,
+                                double damping = 0.85, double tol = 1e-4) {
     Matrix<float>* AT = G->AT;
     Vector<Index>* d_out = G->coldegree;
     Descriptor desc;

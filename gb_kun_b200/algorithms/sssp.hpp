@@ -4,8 +4,8 @@
 // (integer weights below 2^24 are exact in float); T = int runs with int32
 // weights and saturating additions.
 //
-//  * sssp_bellman_ford_blast runs a label-correcting worklist on the device
-//    (gbk_sssp_dist, one graph launch for all rounds).  Each distance is the
+//  * sssp_bellman_ford_blast runs a label-correcting near-far worklist on the
+//    device (gbk_sssp_dist, one graph launch for all rounds).  Each distance is the
 //    minimum over walks of the left-to-right rounded sums either way, since
 //    rounding is monotone, so the result equals the reference's.
 //  * sssp_bellman_ford_blast_ops is the reference's own sequence: every
@@ -27,7 +27,8 @@ template <typename T>
 Index sssp_bellman_ford_blast(Vector<T>* v, const Matrix<T>* A, Index s, Descriptor* desc) {
     (void)desc;
     int32_t rounds = 0;
-    throw_if(gbk_sssp_dist(A->handle(), (int64_t)s, v->dense_ptr(), &rounds, stream()), "sssp_bellman_ford_blast");
+    throw_if(gbk_sssp_dist(A->handle(), (int64_t)s, 0.0, v->dense_ptr(), &rounds, stream()),
+             "sssp_bellman_ford_blast");
     return rounds;
 }
 

@@ -136,7 +136,8 @@ def _declare(lib):
         "gbk_bfs_levels": ([vp, i64, ci, ci, vp, C.POINTER(i32), vp], ci),
         "gbk_matrix_pattern_symmetric": ([vp, C.POINTER(i32), vp], ci),
         "gbk_cc_labels": ([vp, ci, vp, vp], ci),
-        "gbk_sssp_dist": ([vp, i64, vp, C.POINTER(i32), vp], ci),
+        "gbk_sssp_dist": ([vp, i64, C.c_double, vp, C.POINTER(i32), vp], ci),
+        "gbk_pagerank": ([vp, i32, C.c_double, C.c_double, vp, C.POINTER(i32), C.POINTER(C.c_float), vp], ci),
         "gbk_batch_autotune": ([vp, ci, vp, ci, C.POINTER(BatchTuneResult), vp], ci),
         "gbk_mxm": ([C.POINTER(vp), vp, vp, ci, vp], ci),
         "gbk_triangle_count": ([vp, C.POINTER(C.c_uint64), vp], ci),
@@ -395,13 +396,22 @@ class Matrix:
                                    C.byref(depth), stream_ptr(stream)), "gbk_bfs_levels")
         return depth.value
 
-    def sssp(self, source, dist, stream=None):
+    def sssp(self, source, dist, delta=0.0, stream=None):
         """Shortest-path distances from source into dist (device, n elements of the matrix's value
-        type: float32 with FLT_MAX or int32 with INT32_MAX for unreachable).  Returns the rounds run."""
+        type: float32 with FLT_MAX or int32 with INT32_MAX for unreachable).  delta: near-far
+        threshold step (0 automatic, < 0 plain worklist).  Returns the rounds run."""
         rounds = C.c_int32(0)
-        check(lib().gbk_sssp_dist(self.h, int(source), ptr(dist), C.byref(rounds), stream_ptr(stream)),
-              "gbk_sssp_dist")
+        check(lib().gbk_sssp_dist(self.h, int(source), float(delta), ptr(dist), C.byref(rounds),
+                                  stream_ptr(stream)), "gbk_sssp_dist")
         return rounds.value
+
+    def pagerank(self, ranks, itermax=100, damping=0.85, tol=1e-6, stream=None):
+        """page_rank_sinks ranks into ranks (device float32, n).  Returns (iterations, last rdiff)."""
+        it = C.c_int32(0)
+        rd = C.c_float(0)
+        check(lib().gbk_pagerank(self.h, int(itermax), float(damping), float(tol), ptr(ranks), C.byref(it),
+                                 C.byref(rd), stream_ptr(stream)), "gbk_pagerank")
+        return it.value, rd.value
 
     def pattern_symmetric(self, stream=None) -> bool:
         """True when the matrix equals its transpose in pattern (rows sorted)."""

@@ -62,6 +62,8 @@ struct gbk_matrix_s {
     gbk::CsrView csc;           // A^T (built lazily)
     bool has_csc = false;
     int8_t pattern_symmetric = -1;  // -1 unknown; gbk_matrix_pattern_symmetric
+    int32_t* coldeg = nullptr;      // entries per column, built by the first gbk_pagerank
+    int64_t coldeg_zero = 0;        // columns without entries (valid with coldeg)
     gbk_format format = GBK_FMT_CSR;
     gbk_format_params params{};
     gbk::SellC* sell[2] = {nullptr, nullptr};

@@ -267,6 +267,23 @@ int gbk_lablas_pagerank(gbk_lablas_graph g, int32_t itermax, double damping, dou
     });
 }
 
+int gbk_lablas_pagerank_ops(gbk_lablas_graph g, int32_t itermax, double damping, double tol, float* ranks,
+                        int32_t* iterations, double* ms) {
+    if (!g || !ranks) return GBK_NULL_POINTER;
+    return guarded([&] {
+        auto* A = g->pagerank_matrix();
+        LAGraph_Graph<float> graph(*A);
+        lablas::Vector<float> r(g->n);
+        int iters = 0;
+        Timer t(ms);
+        lablas::algorithm::page_rank_sinks_ops(&r, &graph, &iters, itermax, damping, tol);
+        t.stop();
+        if (iterations) *iterations = iters;
+        copy_out(r, ranks);
+        return 0;
+    });
+}
+
 int gbk_lablas_ppr(gbk_lablas_graph g, int64_t seed, int32_t itermax, double damping, double tol, float* ranks,
                    int32_t* iterations, double* ms) {
     if (!g || !ranks) return GBK_NULL_POINTER;

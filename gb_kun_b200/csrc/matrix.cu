@@ -211,6 +211,7 @@ int gbk_matrix_destroy(gbk_matrix A) {
     free_view(A->csr);
     free_view(A->csc);
     cudaFree(A->xcopy);
+    cudaFree(A->coldeg);
     delete A;
     return GBK_SUCCESS;
 }

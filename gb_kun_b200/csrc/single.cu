@@ -18,10 +18,16 @@
 //    the level's kernels form the body of one CUDA graph whose `while` node
 //    the control kernel drives, so a whole BFS is one graph launch.
 //  * gbk_sssp_dist: the distances of sssp_bellman_ford_blast by a
-//    label-correcting worklist: each round relaxes the out-edges of the
-//    vertices whose distance dropped in the round before (an atomic min per
-//    edge, a bitmap so each improved vertex is queued once), one graph
-//    launch for all rounds.
+//    label-correcting near-far worklist: each round relaxes the out-edges
+//    of the near vertices whose distance dropped (an atomic min per edge,
+//    bitmaps so each improved vertex is queued once), one graph launch for
+//    all rounds.
+//  * gbk_pagerank: page_rank_sinks (algorithms/pr/pr.hpp:20-153): each
+//    iteration is the matrix's SpMV (plus-second, its autotuned format), one
+//    element-wise pass (teleport, |r_old - r_new|, the next r ./ d and the
+//    sink sum, per-block partials) and a one-block control kernel summing
+//    the partials in a fixed order; the iterations after the first run as
+//    one CUDA graph.
 //  * gbk_cc_labels: connected components as min-vertex-id labels (the fixed
 //    point FastSV reaches on an undirected graph) by lock-free union-find
 //    with sampled linking (Sutton, Ben-Nun and Barak, "Optimizing Parallel
@@ -392,14 +398,34 @@ __global__ void k_levels_out(const int32_t* __restrict__ lv, int64_t n, T* __res
 }
 
 // ---- SSSP -------------------------------------------------------------------
+//
+// Near-far worklist (Davidson, Baxter, Garland and Owens, "Work-Efficient
+// Parallel GPU Methods for Single-Source Shortest Paths", IPDPS 2014): a
+// vertex whose distance drops below the threshold joins the next round's
+// (near) queue, one at or above it joins the far pile; when the near queue
+// runs dry the threshold moves up by delta (or to the smallest far distance
+// plus delta) and a split round moves the far vertices below it into the
+// near queue.  Every improved vertex is expanded again later whatever its
+// pile, so the fixpoint, and with it every distance, is the one plain
+// Bellman-Ford reaches; the threshold only orders the work.
 
+template <typename T>
 struct Sssp1State {
-    int32_t round;
-    int32_t cur;
-    int32_t fcount;
-    int32_t ncount;
+    int32_t round;       // rounds run (expansions and splits)
+    int32_t cur;         // which near queue is the current one
+    int32_t fcount;      // vertices in the current near queue
+    int32_t ncount;      // vertices appended to the next near queue
     int32_t max_rounds;
     int32_t nchunks;
+    int32_t mode;        // 0 expand the near queue, 1 split the far pile
+    int32_t fcur;        // which far buffer holds the pile
+    int32_t farcount;    // vertices in the pile
+    int32_t farnext;     // vertices kept by the running split
+    int32_t use_far;     // 0: plain worklist (every improved vertex is near)
+    T thr;               // near = distance below thr
+    T thr_prev;          // the threshold before the running split
+    T delta;
+    T far_min;           // smallest distance kept in the pile by the running split
 };
 
 template <typename T>
@@ -410,7 +436,9 @@ struct Sssp1Bufs {
     int64_t n;
     T* dist;
     int32_t* q[2];
-    uint32_t* bm[2];
+    uint32_t* bm[2];     // queued-in-this-round marks of the next near queue
+    int32_t* far[2];
+    uint32_t* fbm;       // in-the-pile marks
     int64_t nwords;
     Chunk* chunks;
 };
@@ -424,6 +452,11 @@ __device__ __forceinline__ bool atomic_min_improves(float* p, float d) {
 }
 __device__ __forceinline__ bool atomic_min_improves(int32_t* p, int32_t d) { return atomicMin(p, d) > d; }
 
+__device__ __forceinline__ bool test_and_set(uint32_t* bm, int32_t v) {
+    const uint32_t bit = 1u << (v & 31);
+    return !(atomicOr(bm + (v >> 5), bit) & bit);
+}
+
 template <typename T>
 struct SsspRelax {
     using V = T;
@@ -433,64 +466,130 @@ struct SsspRelax {
     int32_t* qn;
     uint32_t* bn;
     int32_t* ncount;
+    int32_t* far;
+    uint32_t* fbm;
+    int32_t* farcount;
+    T thr;
+    bool use_far;
 
     __device__ V load(int32_t u) const { return __ldcg(dist + u); }
     __device__ __forceinline__ void edge(bool valid, V du, int32_t e) {
         int32_t v = -1;
-        bool found = false;
+        bool near = false, pile = false;
         if (valid) {
             v = col[e];
             const T nd = elem_add(du, w[e]);
             if (nd < __ldcg(dist + v) && atomic_min_improves(dist + v, nd)) {
-                const uint32_t bit = 1u << (v & 31);
-                found = !(atomicOr(bn + (v >> 5), bit) & bit);  // queued once per round
+                if (!use_far || nd < thr)
+                    near = test_and_set(bn, v);  // queued once per round
+                else
+                    pile = test_and_set(fbm, v);  // in the pile once
             }
         }
-        queue_append(found, v, qn, ncount);
+        queue_append(near, v, qn, ncount);
+        queue_append(pile, v, far, farcount);
     }
 };
 
 template <typename T>
-__device__ __forceinline__ SsspRelax<T> sssp_relax(const Sssp1Bufs<T>& b, Sssp1State* st) {
-    return SsspRelax<T>{b.col, b.w, b.dist, b.q[st->cur ^ 1], b.bm[st->round & 1], &st->ncount};
+__device__ __forceinline__ SsspRelax<T> sssp_relax(const Sssp1Bufs<T>& b, Sssp1State<T>* st) {
+    return SsspRelax<T>{b.col,           b.w, b.dist, b.q[st->cur ^ 1], b.bm[st->round & 1], &st->ncount,
+                        b.far[st->fcur], b.fbm, &st->farcount, st->thr, st->use_far != 0};
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kT) k_sssp1_light(Sssp1Bufs<T> b, Sssp1State* st) {
-    SsspRelax<T> op = sssp_relax(b, st);
-    uint32_t* bz = b.bm[(st->round + 1) & 1];  // next round's bitmap, cleared now
+__device__ __forceinline__ void atomic_min_value(T* p, T v) {
+    atomic_min_improves(p, v);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kT) k_sssp1_light(Sssp1Bufs<T> b, Sssp1State<T>* st) {
+    uint32_t* bz = b.bm[(st->round + 1) & 1];  // next round's marks, cleared now
     const int64_t tid = (int64_t)blockIdx.x * kT + threadIdx.x, nth = (int64_t)gridDim.x * kT;
     for (int64_t i = tid; i < b.nwords; i += nth) bz[i] = 0;
-    expand_light(b.q[st->cur], st->fcount, b.rp, b.chunks, &st->nchunks, op);
+    if (st->mode == 0) {
+        SsspRelax<T> op = sssp_relax(b, st);
+        expand_light(b.q[st->cur], st->fcount, b.rp, b.chunks, &st->nchunks, op);
+        return;
+    }
+    // split: the pile's vertices below the old threshold were expanded as
+    // near ones already; below the new one they join the near queue; the
+    // rest stay in the pile
+    const int32_t* fp = b.far[st->fcur];
+    int32_t* fk = b.far[st->fcur ^ 1];
+    int32_t* qn = b.q[st->cur ^ 1];
+    const int32_t fc = st->farcount;
+    const T lo = st->thr_prev, hi = st->thr;
+    T kmin = Lim<T>::max();
+    const int64_t nr = ((int64_t)fc + 31) / 32 * 32;
+    for (int64_t k = tid; k < nr; k += nth) {
+        const int32_t v = k < fc ? fp[k] : -1;
+        bool near = false, keep = false;
+        if (v >= 0) {
+            const T d = __ldcg(b.dist + v);
+            if (d < lo) {
+                atomicAnd(b.fbm + (v >> 5), ~(1u << (v & 31)));
+            } else if (d < hi) {
+                atomicAnd(b.fbm + (v >> 5), ~(1u << (v & 31)));
+                near = true;
+            } else {
+                keep = true;
+                kmin = d < kmin ? d : kmin;
+            }
+        }
+        queue_append(near, v, qn, &st->ncount);
+        queue_append(keep, v, fk, &st->farnext);
+    }
+    if (kmin < Lim<T>::max()) atomic_min_value(&st->far_min, kmin);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kT) k_sssp1_heavy(Sssp1Bufs<T> b, Sssp1State* st) {
+__global__ void __launch_bounds__(kT) k_sssp1_heavy(Sssp1Bufs<T> b, Sssp1State<T>* st) {
+    if (st->mode != 0) return;
     SsspRelax<T> op = sssp_relax(b, st);
     expand_heavy(b.chunks, st->nchunks, b.rp, op);
 }
 
-__global__ void k_sssp1_control(Sssp1State* st, cudaGraphConditionalHandle h) {
+template <typename T>
+__global__ void k_sssp1_control(Sssp1State<T>* st, cudaGraphConditionalHandle h) {
     if (threadIdx.x != 0) return;
+    if (st->mode == 1) {  // a split ended: the kept vertices are the pile
+        st->farcount = st->farnext;
+        st->farnext = 0;
+        st->fcur ^= 1;
+    }
     const int32_t nc = st->ncount;
-    const bool cont = nc > 0 && st->round < st->max_rounds;
-    if (cont) {
+    bool cont = st->round < st->max_rounds;
+    if (nc > 0) {
+        st->mode = 0;
         st->fcount = nc;
         st->cur ^= 1;
-        st->round += 1;
+    } else if (st->farcount > 0) {
+        // the near queue ran dry: raise the threshold past the smallest
+        // distance in the pile (known after a split) and split
+        const T base = st->mode == 1 ? st->far_min : st->thr;
+        st->thr_prev = st->thr;
+        const T t = elem_add(base, st->delta);  // saturates for int32
+        st->thr = t > base ? t : Lim<T>::max();
+        st->mode = 1;
+        st->far_min = Lim<T>::max();
+    } else {
+        cont = false;
     }
+    if (cont) st->round += 1;
     st->ncount = 0;
     st->nchunks = 0;
     cudaGraphSetConditional(h, cont ? 1u : 0u);
 }
 
 template <typename T>
-__global__ void k_sssp1_init(Sssp1Bufs<T> b, Sssp1State* st, int32_t src) {
+__global__ void k_sssp1_init(Sssp1Bufs<T> b, Sssp1State<T>* st, int32_t src, T delta, int use_far) {
     const int64_t tid = (int64_t)blockIdx.x * kT + threadIdx.x, nth = (int64_t)gridDim.x * kT;
     for (int64_t i = tid; i < b.n; i += nth) b.dist[i] = i == src ? T(0) : Lim<T>::max();
     for (int64_t i = tid; i < b.nwords; i += nth) {
         b.bm[0][i] = 0;
         b.bm[1][i] = 0;
+        b.fbm[i] = 0;
     }
     if (tid == 0) {
         b.q[0][0] = src;
@@ -498,14 +597,40 @@ __global__ void k_sssp1_init(Sssp1Bufs<T> b, Sssp1State* st, int32_t src) {
         st->cur = 0;
         st->fcount = 1;
         st->ncount = 0;
-        st->max_rounds = b.n < (int64_t)INT32_MAX ? (int32_t)b.n : INT32_MAX;
+        st->max_rounds = b.n < (int64_t)INT32_MAX / 2 ? 2 * (int32_t)b.n + 1 : INT32_MAX;
         st->nchunks = 0;
+        st->mode = 0;
+        st->fcur = 0;
+        st->farcount = 0;
+        st->farnext = 0;
+        st->use_far = use_far;
+        st->delta = delta;
+        st->thr = delta;
+        st->thr_prev = T(0);
+        st->far_min = Lim<T>::max();
+    }
+}
+
+// Mean of up to 65536 evenly spaced entries of w (one block).
+template <typename T>
+__global__ void __launch_bounds__(1024) k_sample_mean(const T* __restrict__ w, int64_t nnz, double* out) {
+    __shared__ double red[32];
+    const int64_t m = nnz < 65536 ? nnz : 65536;
+    double s = 0.0;
+    for (int64_t k = threadIdx.x; k < m; k += 1024) s += (double)w[k * nnz / m];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(kAll, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = red[threadIdx.x];
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(kAll, s, o);
+        if (threadIdx.x == 0) *out = m > 0 ? s / (double)m : 0.0;
     }
 }
 
 template <typename T>
-int run_sssp1(gbk_matrix A, int32_t source, T* dist, int32_t* rounds, cudaStream_t s) {
-    const int64_t n = A->csr.nrows;
+int run_sssp1(gbk_matrix A, int32_t source, double delta, T* dist, int32_t* rounds, cudaStream_t s) {
+    const int64_t n = A->csr.nrows, nnz = A->csr.nnz;
     Sssp1Bufs<T> b{};
     b.rp = A->csr.ptr;
     b.col = A->csr.idx;
@@ -515,36 +640,195 @@ int run_sssp1(gbk_matrix A, int32_t source, T* dist, int32_t* rounds, cudaStream
     b.dist = dist;
     void* mem = nullptr;
     const size_t st_b = 256, q_b = 4 * (size_t)n, bm_b = 4 * (size_t)b.nwords,
-                 ch_b = sizeof(Chunk) * (size_t)max_chunks(A->csr.nnz);
-    GBK_CUDA(cudaMallocAsync(&mem, st_b + ch_b + 2 * q_b + 2 * bm_b, s));
+                 ch_b = sizeof(Chunk) * (size_t)max_chunks(nnz);
+    GBK_CUDA(cudaMallocAsync(&mem, st_b + ch_b + 4 * q_b + 3 * bm_b, s));
     char* m = (char*)mem;
-    Sssp1State* st = (Sssp1State*)m;
+    Sssp1State<T>* st = (Sssp1State<T>*)m;
     b.chunks = (Chunk*)(m + st_b);
     m += st_b + ch_b;
     b.q[0] = (int32_t*)m;
     b.q[1] = (int32_t*)(m + q_b);
-    b.bm[0] = (uint32_t*)(m + 2 * q_b);
-    b.bm[1] = (uint32_t*)(m + 2 * q_b + bm_b);
+    b.far[0] = (int32_t*)(m + 2 * q_b);
+    b.far[1] = (int32_t*)(m + 3 * q_b);
+    b.bm[0] = (uint32_t*)(m + 4 * q_b);
+    b.bm[1] = (uint32_t*)(m + 4 * q_b + bm_b);
+    b.fbm = (uint32_t*)(m + 4 * q_b + 2 * bm_b);
+    int rc = GBK_SUCCESS;
+    auto fail = [&](cudaError_t e, const char* what) {
+        if (rc == GBK_SUCCESS && e != cudaSuccess) rc = cuda_fail(e, what, __FILE__, __LINE__);
+    };
+    if (delta == 0.0 && nnz > 0) {
+        // 8 x mean weight / mean row length (R-MAT scale 23 with weights in
+        // [1, 255]: 10.1 ms at 8x, 10.8 ms at 32x, 11.4 ms without the pile)
+        double* mean = (double*)st;  // the state is written after this
+        k_sample_mean<T><<<1, 1024, 0, s>>>(b.w, nnz, mean);
+        count_launch(1);
+        double h = 0.0;
+        fail(cudaMemcpyAsync(&h, mean, sizeof(h), cudaMemcpyDeviceToHost, s), "SSSP weight sample");
+        fail(cudaStreamSynchronize(s), "SSSP weight sample");
+        delta = h > 0.0 ? 8.0 * h * (double)n / (double)nnz : -1.0;
+    }
+    const bool use_far = delta > 0.0;
+    T dl = T(1);
+    if (use_far) {
+        if (std::is_integral<T>::value)
+            dl = (T)std::min(std::max(delta, 1.0), (double)INT32_MAX / 2);
+        else
+            dl = (T)std::min(delta, 1e30);
+    }
     const int grid = blocks_for_sm((const void*)k_sssp1_light<T>);
-    k_sssp1_init<T><<<grid, kT, 0, s>>>(b, st, source);
-    cudaError_t e = cudaGetLastError();
-    int rc = e == cudaSuccess ? GBK_SUCCESS : cuda_fail(e, "k_sssp1_init", __FILE__, __LINE__);
-    count_launch(1);
+    if (rc == GBK_SUCCESS) {
+        k_sssp1_init<T><<<grid, kT, 0, s>>>(b, st, source, dl, use_far ? 1 : 0);
+        fail(cudaGetLastError(), "k_sssp1_init");
+        count_launch(1);
+    }
     if (rc == GBK_SUCCESS)
         rc = run_loop_graph(s, [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
             k_sssp1_light<T><<<grid, kT, 0, cs>>>(b, st);
             k_sssp1_heavy<T><<<grid, kT, 0, cs>>>(b, st);
-            k_sssp1_control<<<1, 32, 0, cs>>>(st, h);
+            k_sssp1_control<T><<<1, 32, 0, cs>>>(st, h);
         });
     if (rc == GBK_SUCCESS && rounds) {
-        Sssp1State h{};
-        e = cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) rc = cuda_fail(e, "SSSP rounds", __FILE__, __LINE__);
+        Sssp1State<T> h{};
+        fail(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s), "SSSP rounds");
+        fail(cudaStreamSynchronize(s), "SSSP rounds");
         *rounds = h.round;
     }
     cudaFreeAsync(mem, s);
     return rc;
+}
+
+// ---- PageRank ---------------------------------------------------------------
+
+struct PrState {
+    int32_t iters;
+    int32_t itermax;
+    int32_t cur;       // which rank buffer holds the current ranks
+    int32_t cont;
+    float tol;
+    float scaled;      // (1 - damping) / n
+    float d_over_n;    // damping / n
+    float sink;        // sum of the current ranks over the sinks
+    float rdiff;       // sum |old - new| of the last iteration
+};
+
+struct PrBufs {
+    int64_t n;
+    const int32_t* deg;  // entries per column of A
+    float* r[2];
+    float* w;            // r ./ d, the SpMV input
+    float* y;            // A w
+    float* part_sink;    // per-block partial sums
+    float* part_diff;
+    float damping;
+    float inv_damping;   // 1 / damping
+    int64_t nsinks;      // columns without entries
+    int sparse_sink;     // 1: the sink mass is the sum of the first nsinks ranks
+};
+
+// The sink mass as the reference forms it: its sink vector, built by a
+// masked assign, turns sparse when it holds at most 0.3 n entries, and its
+// masked assign from a sparse mask then reads the ranks at the mask-list
+// positions 0 .. nsinks - 1 instead of at the sinks' ids
+// (src/backend/operations/generic_operations.h:28-34 with operations.h:63-65).
+__device__ __forceinline__ bool pr_sink_term(const PrBufs& b, int64_t i, int32_t deg) {
+    return b.sparse_sink ? i < b.nsinks : deg == 0;
+}
+
+// d = max(deg / damping, 1 / damping), in float as the reference computes it
+__device__ __forceinline__ float pr_d(const PrBufs& b, int32_t deg) {
+    return fmaxf((float)deg / b.damping, b.inv_damping);
+}
+
+template <int NT>
+__device__ __forceinline__ float block_sum(float v) {
+    __shared__ float red[NT / 32];
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kAll, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    float t = 0.0f;
+    if (threadIdx.x < 32) {
+        t = threadIdx.x < NT / 32 ? red[threadIdx.x] : 0.0f;
+        for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(kAll, t, o);
+    }
+    __syncthreads();
+    return t;  // valid in thread 0
+}
+
+// r0 = 1 / n, w = r0 ./ d, partial sums of r0 over the sinks
+__global__ void __launch_bounds__(kT) k_pr_init(PrBufs b, float r0) {
+    float sink = 0.0f;
+    for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < b.n; i += (int64_t)gridDim.x * kT) {
+        const int32_t dg = b.deg[i];
+        b.r[0][i] = r0;
+        b.w[i] = r0 / pr_d(b, dg);
+        if (pr_sink_term(b, i, dg)) sink += r0;
+    }
+    sink = block_sum<kT>(sink);
+    if (threadIdx.x == 0) {
+        b.part_sink[blockIdx.x] = sink;
+        b.part_diff[blockIdx.x] = 0.0f;
+    }
+}
+
+// r_new = teleport + y with teleport = (1 - damping) / n + damping / n * (sum of
+// the old ranks over the sinks); partial sums of |r_old - r_new| and of the
+// new ranks over the sinks; w = r_new ./ d for the next product
+__global__ void __launch_bounds__(kT) k_pr_post(PrBufs b, const PrState* st) {
+    const float teleport = st->scaled + st->d_over_n * st->sink;
+    const float* __restrict__ ro = b.r[st->cur];
+    float* __restrict__ rn = b.r[st->cur ^ 1];
+    float sink = 0.0f, diff = 0.0f;
+    for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < b.n; i += (int64_t)gridDim.x * kT) {
+        const int32_t dg = b.deg[i];
+        const float r = teleport + b.y[i];
+        diff += fabsf(ro[i] - r);
+        rn[i] = r;
+        b.w[i] = r / pr_d(b, dg);
+        if (pr_sink_term(b, i, dg)) sink += r;
+    }
+    sink = block_sum<kT>(sink);
+    diff = block_sum<kT>(diff);
+    if (threadIdx.x == 0) {
+        b.part_sink[blockIdx.x] = sink;
+        b.part_diff[blockIdx.x] = diff;
+    }
+}
+
+// Sums the partials in a fixed order (the same result every run), counts
+// the iteration (iter = 1) and decides whether another one runs.
+__global__ void __launch_bounds__(256) k_pr_control(PrBufs b, PrState* st, int nparts, int iter,
+                                                    cudaGraphConditionalHandle h) {
+    float s = 0.0f, d = 0.0f;
+    for (int i = threadIdx.x; i < nparts; i += 256) {
+        s += b.part_sink[i];
+        d += b.part_diff[i];
+    }
+    s = block_sum<256>(s);
+    d = block_sum<256>(d);
+    if (threadIdx.x == 0) {
+        st->sink = s;
+        if (iter) {
+            st->rdiff = d;
+            st->iters += 1;
+            st->cur ^= 1;
+        }
+        const bool cont = st->iters < st->itermax && !(st->tol > 0.0f && st->rdiff < st->tol);
+        st->cont = cont ? 1 : 0;
+        if (h) cudaGraphSetConditional(h, cont ? 1u : 0u);
+    }
+}
+
+__global__ void k_col_degree(const int32_t* __restrict__ col, int64_t nnz, int32_t* deg) {
+    for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < nnz; i += (int64_t)gridDim.x * kT)
+        atomicAdd(deg + col[i], 1);
+}
+
+__global__ void k_count_zero(const int32_t* __restrict__ deg, int64_t n, unsigned long long* count) {
+    unsigned c = 0;
+    for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)gridDim.x * kT) c += deg[i] == 0;
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(kAll, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
 }
 
 // ---- CC ---------------------------------------------------------------------
@@ -766,15 +1050,125 @@ extern "C" int gbk_bfs_levels(gbk_matrix A, int64_t source, int direction, gbk_d
     return rc;
 }
 
-extern "C" int gbk_sssp_dist(gbk_matrix A, int64_t source, void* dist, int32_t* rounds, void* stream) {
+extern "C" int gbk_sssp_dist(gbk_matrix A, int64_t source, double delta, void* dist, int32_t* rounds,
+                             void* stream) {
     GBK_REQUIRE(A && dist, GBK_NULL_POINTER, "gbk_sssp_dist: NULL argument");
     const int64_t n = A->csr.nrows;
     GBK_REQUIRE(A->csr.ncols == n, GBK_DIMENSION_MISMATCH, "gbk_sssp_dist: the matrix must be square");
     GBK_REQUIRE(source >= 0 && source < n, GBK_INVALID_INDEX, "gbk_sssp_dist: source %lld outside [0, %lld)",
                 (long long)source, (long long)n);
     cudaStream_t s = (cudaStream_t)stream;
-    if (A->vtype == GBK_F32) return run_sssp1<float>(A, (int32_t)source, (float*)dist, rounds, s);
-    return run_sssp1<int32_t>(A, (int32_t)source, (int32_t*)dist, rounds, s);
+    if (A->vtype == GBK_F32) return run_sssp1<float>(A, (int32_t)source, delta, (float*)dist, rounds, s);
+    return run_sssp1<int32_t>(A, (int32_t)source, delta, (int32_t*)dist, rounds, s);
+}
+
+extern "C" int gbk_pagerank(gbk_matrix A, int32_t itermax, double damping, double tol, float* ranks,
+                            int32_t* iters, float* rdiff, void* stream) {
+    GBK_REQUIRE(A && ranks, GBK_NULL_POINTER, "gbk_pagerank: NULL argument");
+    const int64_t n = A->csr.nrows;
+    GBK_REQUIRE(A->csr.ncols == n, GBK_DIMENSION_MISMATCH, "gbk_pagerank: the matrix must be square");
+    GBK_REQUIRE(A->vtype == GBK_F32, GBK_DOMAIN_MISMATCH, "gbk_pagerank: the matrix values must be GBK_F32");
+    GBK_REQUIRE(damping > 0.0, GBK_INVALID_VALUE, "gbk_pagerank: damping %g must be positive", damping);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (n == 0) {
+        if (iters) *iters = 0;
+        return GBK_SUCCESS;
+    }
+    if (!A->coldeg) {
+        int32_t* deg = nullptr;
+        GBK_CUDA(cudaMalloc((void**)&deg, 4 * (size_t)n + 16));
+        unsigned long long* zero = (unsigned long long*)(deg + ((n + 1) / 2) * 2);
+        GBK_CUDA(cudaMemsetAsync(deg, 0, 4 * (size_t)n + 16, s));
+        const unsigned g = (unsigned)std::min<int64_t>(grid1(std::max(n, A->csr.nnz)), 8 * num_sms());
+        if (A->csr.nnz > 0) {
+            k_col_degree<<<g, kT, 0, s>>>(A->csr.idx, A->csr.nnz, deg);
+            GBK_LAUNCHED();
+        }
+        k_count_zero<<<g, kT, 0, s>>>(deg, n, zero);
+        GBK_LAUNCHED();
+        unsigned long long hz = 0;
+        GBK_CUDA(cudaMemcpyAsync(&hz, zero, 8, cudaMemcpyDeviceToHost, s));
+        GBK_CUDA(cudaStreamSynchronize(s));
+        A->coldeg = deg;
+        A->coldeg_zero = (int64_t)hz;
+    }
+    const int nb = blocks_for_sm((const void*)k_pr_post);
+    PrBufs b{};
+    b.n = n;
+    b.deg = A->coldeg;
+    b.damping = (float)damping;
+    b.inv_damping = (float)(1.0 / damping);
+    b.nsinks = A->coldeg_zero;
+    b.sparse_sink = A->coldeg_zero <= (int64_t)((double)n * 0.3) ? 1 : 0;
+    void* mem = nullptr;
+    const size_t st_b = 256, v_b = 4 * (size_t)n, p_b = 4 * (size_t)nb;
+    GBK_CUDA(cudaMallocAsync(&mem, st_b + 3 * v_b + 2 * p_b, s));
+    char* m = (char*)mem;
+    PrState* st = (PrState*)m;
+    m += st_b;
+    b.r[0] = ranks;
+    b.r[1] = (float*)m;
+    b.w = (float*)(m + v_b);
+    b.y = (float*)(m + 2 * v_b);
+    b.part_sink = (float*)(m + 3 * v_b);
+    b.part_diff = (float*)(m + 3 * v_b + p_b);
+    PrState h0{};
+    h0.itermax = itermax;
+    h0.tol = (float)tol;
+    h0.scaled = (float)((1.0 - damping) / (double)n);
+    h0.d_over_n = (float)(damping / (double)n);
+    h0.rdiff = 1.0f;
+    int rc = GBK_SUCCESS;
+    auto fail = [&](cudaError_t e, const char* what) {
+        if (rc == GBK_SUCCESS && e != cudaSuccess) rc = cuda_fail(e, what, __FILE__, __LINE__);
+    };
+    fail(cudaMemcpyAsync(st, &h0, sizeof(h0), cudaMemcpyHostToDevice, s), "gbk_pagerank state");
+    if (rc == GBK_SUCCESS) {
+        k_pr_init<<<nb, kT, 0, s>>>(b, (float)(1.0 / (double)n));
+        k_pr_control<<<1, 256, 0, s>>>(b, st, nb, 0, 0);
+        fail(cudaGetLastError(), "k_pr_init");
+        count_launch(2);
+    }
+    // one iteration outside the graph: the first product also builds
+    // whatever the matrix's format builds on first use
+    PrState h{};
+    auto iterate = [&](cudaStream_t cs, cudaGraphConditionalHandle hd) {
+        int r = gbk_mxv(A, 0, GBK_PLUS_SECOND, GBK_OP_SECOND, GBK_F32, b.w, b.y, nullptr, GBK_F32, GBK_MASK_DEFAULT,
+                        cs);
+        k_pr_post<<<nb, kT, 0, cs>>>(b, st);
+        k_pr_control<<<1, 256, 0, cs>>>(b, st, nb, 1, hd);
+        count_launch(2);
+        return r;
+    };
+    if (rc == GBK_SUCCESS) {
+        fail(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s), "gbk_pagerank state");
+        fail(cudaStreamSynchronize(s), "gbk_pagerank state");
+    }
+    if (rc == GBK_SUCCESS && h.cont) {
+        rc = iterate(s, 0);
+        fail(cudaGetLastError(), "PageRank iteration");
+        if (rc == GBK_SUCCESS) {
+            fail(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s), "gbk_pagerank state");
+            fail(cudaStreamSynchronize(s), "gbk_pagerank state");
+        }
+    }
+    if (rc == GBK_SUCCESS && h.cont) {
+        int irc = GBK_SUCCESS;
+        rc = run_loop_graph(s, [&](cudaStream_t cs, cudaGraphConditionalHandle hd) { irc = iterate(cs, hd); });
+        if (rc == GBK_SUCCESS) rc = irc;
+        if (rc == GBK_SUCCESS) {
+            fail(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s), "gbk_pagerank state");
+            fail(cudaStreamSynchronize(s), "gbk_pagerank state");
+        }
+    }
+    if (rc == GBK_SUCCESS && h.cur == 1)
+        fail(cudaMemcpyAsync(ranks, b.r[1], v_b, cudaMemcpyDeviceToDevice, s), "gbk_pagerank ranks");
+    if (rc == GBK_SUCCESS) {
+        if (iters) *iters = h.iters;
+        if (rdiff) *rdiff = h.rdiff;
+    }
+    cudaFreeAsync(mem, s);
+    return rc;
 }
 
 extern "C" int gbk_matrix_pattern_symmetric(gbk_matrix A, int32_t* symmetric, void* stream) {

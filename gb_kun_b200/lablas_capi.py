@@ -40,6 +40,7 @@ def lib():
         L.gbk_lablas_sssp_f32_ops.argtypes = [vp, i64, vp, dp]
         L.gbk_lablas_sssp_i32.argtypes = [vp, i64, vp, dp]
         L.gbk_lablas_pagerank.argtypes = [vp, i32, C.c_double, C.c_double, vp, C.POINTER(i32), dp]
+        L.gbk_lablas_pagerank_ops.argtypes = [vp, i32, C.c_double, C.c_double, vp, C.POINTER(i32), dp]
         L.gbk_lablas_ppr.argtypes = [vp, i64, i32, C.c_double, C.c_double, vp, C.POINTER(i32), dp]
         L.gbk_lablas_tc.argtypes = [vp, C.POINTER(C.c_uint64), dp]
         L.gbk_lablas_tc_method.argtypes = [vp, i32, C.POINTER(C.c_uint64), dp]
@@ -149,6 +150,14 @@ class Graph:
         ms = C.c_double()
         _check(lib().gbk_lablas_pagerank(self.h, itermax, damping, tol, _p(out), C.byref(it), C.byref(ms)),
                "pagerank")
+        return out, it.value, ms.value
+
+    def pagerank_ops(self, itermax=100, damping=0.85, tol=0.0):
+        out = np.empty(self.n, np.float32)
+        it = C.c_int32()
+        ms = C.c_double()
+        _check(lib().gbk_lablas_pagerank_ops(self.h, itermax, damping, tol, _p(out), C.byref(it), C.byref(ms)),
+               "pagerank_ops")
         return out, it.value, ms.value
 
     def ppr(self, seed, itermax=100, damping=0.85, tol=1e-6):

@@ -281,14 +281,39 @@ int gbk_bfs_levels(gbk_matrix A, int64_t source, int direction, gbk_dtype level_
  * right in the matrix's value type (GBK_F32: float, FLT_MAX = unreachable;
  * GBK_I32: saturating int32, INT32_MAX = unreachable); dist[source] = 0.
  * dist is device memory of n elements of the matrix's value type.  A
- * label-correcting worklist: each round relaxes the out-edges (rows of A) of
- * the vertices whose distance dropped in the round before; all rounds run as
- * one CUDA graph with a device-side `while` node.  Negative edge values are
- * allowed; with a negative cycle reachable the rounds stop after n and the
- * distances are not defined (the reference's n-round bound gives other
- * values there).  rounds (host, may be NULL) receives the rounds run and then
- * the call synchronises the stream; with rounds NULL it does not. */
-int gbk_sssp_dist(gbk_matrix A, int64_t source, void* dist, int32_t* rounds, void* stream);
+ * label-correcting near-far worklist: each round relaxes the out-edges (rows
+ * of A) of the vertices whose distance dropped below a threshold; vertices at
+ * or above it wait in a far pile until the threshold rises by delta.  delta
+ * 0 picks 8 x the mean edge value / the mean row length (sampled), delta < 0
+ * turns the pile off (plain worklist); the distances are the same either way.
+ * All rounds run as one CUDA graph with a device-side `while` node.  Negative
+ * edge values are allowed; with a negative cycle reachable the rounds stop
+ * after 2n + 1 and the distances are not defined (the reference's n-round
+ * bound gives other values there).  rounds (host, may be NULL) receives the
+ * rounds run and then the call synchronises the stream; with rounds NULL and
+ * delta != 0 it does not. */
+int gbk_sssp_dist(gbk_matrix A, int64_t source, double delta, void* dist, int32_t* rounds, void* stream);
+/* PageRank as page_rank_sinks (algorithms/pr/pr.hpp:20-153) on the graph
+ * whose edge j -> i is the entry a_ij (the reference's AT): r0 = 1/n; each
+ * iteration r = teleport + A (r_old ./ d) with d = max(coldeg / damping,
+ * 1 / damping) in float (coldeg = entries in the column), teleport =
+ * (1 - damping) / n + damping / n * sink, where sink is the reference's sink
+ * mass: the sum of r_old over the columns without entries when there are
+ * more than 0.3 n of them, and otherwise the sum of r_old[0 .. nsinks - 1]
+ * (its sparse sink vector is read at list positions, not at vertex ids:
+ * src/backend/operations/generic_operations.h:28-34 with operations.h:63-65).
+ * The loop stops after itermax iterations, or earlier once
+ * sum |r_old - r| < tol when tol > 0.  A's values must be GBK_F32 (they are
+ * not read: plus-second).  ranks is device memory of n floats.  The SpMV runs
+ * in A's storage format (gbk_matrix_set_format / gbk_matrix_autotune); after
+ * the first iteration the loop runs as one CUDA graph.  The element-wise
+ * sums are formed in a fixed order, so with the CSR format a run repeats bit
+ * for bit; the staged formats fold row pieces with atomics, whose order can
+ * move the last bits between runs.  iters and rdiff
+ * (host, may be NULL) receive the iterations run and the last sum
+ * |r_old - r|.  Synchronises the stream. */
+int gbk_pagerank(gbk_matrix A, int32_t itermax, double damping, double tol, float* ranks, int32_t* iters,
+                 float* rdiff, void* stream);
 /* *symmetric = 1 when A is square and its pattern equals its transpose's with
  * every row's column indices ascending, else 0 (an unsorted symmetric matrix
  * reads as 0).  Computed once per matrix on the device against its CSC. */

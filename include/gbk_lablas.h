@@ -58,6 +58,10 @@ int gbk_lablas_sssp_i32(gbk_lablas_graph g, int64_t source, int32_t* dist, doubl
  * itermax iterations or once rdiff < tol (tol > 0). */
 int gbk_lablas_pagerank(gbk_lablas_graph g, int32_t itermax, double damping, double tol, float* ranks,
                         int32_t* iterations, double* ms);
+/* The same iteration as page_rank_sinks' own sequence of GraphBLAS calls
+ * (a host read of rdiff per iteration). */
+int gbk_lablas_pagerank_ops(gbk_lablas_graph g, int32_t itermax, double damping, double tol, float* ranks,
+                        int32_t* iterations, double* ms);
 /* Personalised PageRank from one seed through the same lablas:: steps
  * (one plus-second mxv per iteration); teleport and sink mass return to the
  * seed.  The single-query path the batched gbk_ppr is compared with. */

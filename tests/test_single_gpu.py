@@ -266,8 +266,9 @@ def test_sssp_golden(torch, golden, name):
     A.close()
 
 
+@pytest.mark.parametrize("delta", [0.0, -1.0, 1.0, 300.0, 1e9], ids=["auto", "plain", "d1", "d300", "dhuge"])
 @pytest.mark.parametrize("undirected", [True, False])
-def test_sssp_int_vs_oracle(torch, oracle, undirected):
+def test_sssp_int_vs_oracle(torch, oracle, undirected, delta):
     from gb_kun_b200 import capi
     g = gg.rmat(15, 16, seed=51, undirected=undirected)
     w = gg.weights_i32(g, seed=52)
@@ -275,20 +276,21 @@ def test_sssp_int_vs_oracle(torch, oracle, undirected):
     d = torch.zeros(g.n, dtype=torch.int32, device="cuda")
     deg = np.diff(g.row_ptr)
     for s in [int(x) for x in gg.sources(g, 3, seed=53)] + [int(np.argmax(deg))]:
-        A.sssp(s, d)
+        A.sssp(s, d, delta=delta)
         want = oracle.sssp(g, w, s)
         assert np.array_equal(d.cpu().numpy(), np.where(want < 0, np.iinfo(np.int32).max, want).astype(np.int32)), s
     A.close()
 
 
-def test_sssp_float_weights_vs_dijkstra(torch):
+@pytest.mark.parametrize("delta", [0.0, -1.0, 0.37], ids=["auto", "plain", "d037"])
+def test_sssp_float_weights_vs_dijkstra(torch, delta):
     from gb_kun_b200 import capi
     g = gg.rmat(11, 8, seed=61)
     w = (np.random.default_rng(62).random(g.nnz, dtype=np.float32) * 3.7 + 0.01).astype(np.float32)
     A = capi.Matrix.from_graph(g, w)
     d = torch.zeros(g.n, dtype=torch.float32, device="cuda")
     for s in gg.sources(g, 3, seed=63):
-        A.sssp(int(s), d)
+        A.sssp(int(s), d, delta=delta)
         assert np.array_equal(d.cpu().numpy(), _dijkstra(g, w, int(s), np.float32)), int(s)
     A.close()
 
@@ -304,7 +306,7 @@ def test_sssp_negative_weights_dag(torch):
     w = rng.integers(-20, 100, g.nnz).astype(np.int32)
     A = capi.Matrix.from_graph(g, w)
     d = torch.zeros(n, dtype=torch.int32, device="cuda")
-    A.sssp(0, d)
+    A.sssp(0, d, delta=10.0)
     # Bellman-Ford in topological (id) order is exact on a DAG
     want = np.full(n, np.iinfo(np.int32).max, np.int64)
     want[0] = 0
@@ -345,3 +347,71 @@ def test_lablas_sssp_fused_equals_graphblas_sequence(torch, oracle):
         d64 = oracle.sssp(g, w, int(s))
         assert np.array_equal(a, b)
         assert np.array_equal(a, np.where(d64 < 0, np.finfo(np.float32).max, d64).astype(np.float32))
+
+
+# ---- PageRank ----------------------------------------------------------------
+
+@pytest.mark.parametrize("name", ["rmat11u", "er11u"])
+def test_pagerank_golden(torch, golden, name):
+    from conftest import REL_L1_TOL, rel_l1
+    data, _ = golden
+    g = golden_graph(data, name)
+    A = _mat(g)
+    r = torch.zeros(g.n, device="cuda")
+    for it in (1, 5, 20):
+        n_it, _ = A.pagerank(r, itermax=it, damping=0.85, tol=0.0)
+        assert n_it == it
+        assert rel_l1(r.cpu().numpy(), data[f"{name}.pr.{it}"]) < REL_L1_TOL, (name, it)
+    A.close()
+
+
+@pytest.mark.parametrize("fmt", [("CSR", {}), ("SELL_C", {"seg_staged": 1, "reorder_cols": 1}), ("CSR_SEG", {}),
+                                 ("LAV", {})], ids=["CSR", "SELL_C_staged", "CSR_SEG", "LAV"])
+def test_pagerank_vs_fp64_every_format(torch, oracle, fmt):
+    from conftest import REL_L1_TOL, rel_l1
+    g = gg.rmat(16, 16, seed=91)  # directed: sinks present
+    A = _mat(g)
+    A.set_format(fmt[0], **fmt[1])
+    r = torch.zeros(g.n, device="cuda")
+    it, rd = A.pagerank(r, itermax=100, damping=0.85, tol=1e-6)
+    assert 1 < it < 100 and rd < 1e-6
+    r64, _, _ = oracle.pagerank(g, tol=0.0, itermax=it)
+    assert rel_l1(r.cpu().numpy(), r64) < REL_L1_TOL
+    # the element-wise sums are formed in a fixed order: with the CSR SpMV
+    # (row sums in order) a second run repeats bit for bit; the staged
+    # formats fold row pieces with atomics, so their last bits may move
+    r2 = torch.zeros(g.n, device="cuda")
+    it2 = A.pagerank(r2, itermax=100, damping=0.85, tol=1e-6)[0]
+    if fmt[0] == "CSR":
+        assert it2 == it and torch.equal(r, r2)
+    else:
+        assert abs(it2 - it) <= 1 and rel_l1(r2.cpu().numpy(), r64) < REL_L1_TOL
+    A.close()
+
+
+def test_pagerank_edge_cases(torch):
+    g = gg.rmat(10, 8, seed=92)
+    A = _mat(g)
+    r = torch.zeros(g.n, device="cuda")
+    assert A.pagerank(r, itermax=0)[0] == 0
+    assert np.allclose(r.cpu().numpy(), 1.0 / g.n)
+    A.close()
+    g1 = gg.from_edges(1, [], [])
+    A1 = _mat(g1)
+    r1 = torch.zeros(1, device="cuda")
+    A1.pagerank(r1, itermax=3, tol=0.0)
+    # a single sink: teleport (1 - d) + d * r each iteration keeps r = 1
+    assert abs(float(r1.cpu()[0]) - 1.0) < 1e-6
+    A1.close()
+
+
+def test_lablas_pagerank_fused_equals_graphblas_sequence(torch, oracle):
+    from conftest import REL_L1_TOL, rel_l1
+    from gb_kun_b200 import lablas_capi as lc
+    g = gg.rmat(15, 16, seed=93, undirected=True)
+    G = lc.Graph(g)
+    a, ia, _ = G.pagerank(itermax=100, damping=0.85, tol=1e-6)
+    b, ib, _ = G.pagerank_ops(itermax=100, damping=0.85, tol=1e-6)
+    assert abs(ia - ib) <= 1
+    r64, _, _ = oracle.pagerank(g, tol=0.0, itermax=ia)
+    assert rel_l1(a, r64) < REL_L1_TOL and rel_l1(a, b) < REL_L1_TOL
