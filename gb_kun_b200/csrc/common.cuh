@@ -199,6 +199,13 @@ __device__ __forceinline__ void atomic_min_any(float* p, float v) {
 }
 __device__ __forceinline__ void atomic_min_any(int32_t* p, int32_t v) { atomicMin(p, v); }
 
+// count[key] += 1 for every active lane, one atomic per distinct key in the
+// warp (sorted keys repeat within a warp: hub columns, windows)
+__device__ __forceinline__ void warp_count(int32_t* count, int32_t key) {
+    const unsigned peers = __match_any_sync(__activemask(), key);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(count + key, __popc(peers));
+}
+
 __device__ __forceinline__ void atomic_add_any(float* p, float v) { atomicAdd(p, v); }
 __device__ __forceinline__ void atomic_add_any(int32_t* p, int32_t v) {
     // saturating, like elem_add, so INT_MAX stays the min-plus infinity

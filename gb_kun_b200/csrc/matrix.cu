@@ -60,7 +60,7 @@ __global__ void k_transpose_finish(const unsigned long long* __restrict__ keys, 
     unsigned long long key = keys[k];
     trow[k] = (int32_t)(key & 0xffffffffULL);
     tval[k] = val[pos[k]];
-    atomicAdd(&count[(int32_t)(key >> 32)], 1);
+    warp_count(count, (int32_t)(key >> 32));  // keys sorted by column: one atomic per column per warp
 }
 
 int alloc_carries(CsrView& v, int elem_bytes) {

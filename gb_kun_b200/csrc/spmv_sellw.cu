@@ -96,15 +96,23 @@ int sw_scan_excl(const int32_t* in, int32_t* out, int64_t n, cudaStream_t s) {
 
 // ---- build ------------------------------------------------------------------
 
-// key = (window << 32) | row, value = entry position
-__global__ void k_sw_keys(const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx, int64_t n,
+// key = (window << 32) | row, value = entry position; one thread per entry,
+// its row by binary search in the row pointers (a thread per row would walk
+// a hub row of 10^5 entries alone)
+__global__ void k_sw_keys(const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx, int64_t n, int64_t nnz,
                           unsigned long long* __restrict__ keys, int32_t* __restrict__ pos) {
-    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    for (int32_t e = ptr[r]; e < ptr[r + 1]; ++e) {
-        keys[e] = ((unsigned long long)(idx[e] / kSwCols) << 32) | (unsigned long long)r;
-        pos[e] = e;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    int64_t lo = 0, hi = n;  // largest r with ptr[r] <= e
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (ptr[mid] <= e)
+            lo = mid;
+        else
+            hi = mid;
     }
+    keys[e] = ((unsigned long long)(idx[e] / kSwCols) << 32) | (unsigned long long)lo;
+    pos[e] = (int32_t)e;
 }
 
 // vs[i] = i where a virtual row starts, else 0 (a running max gives each
@@ -140,7 +148,7 @@ __global__ void k_sw_pkey(const int32_t* __restrict__ pfirst, const unsigned lon
 
 __global__ void k_sw_wcount(const uint32_t* __restrict__ pkey_sorted, int64_t np, int32_t* __restrict__ wcnt) {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < np) atomicAdd(wcnt + (pkey_sorted[j] >> 9), 1);
+    if (j < np) warp_count(wcnt, (int32_t)(pkey_sorted[j] >> 9));  // sorted: one atomic per window per warp
 }
 
 __global__ void k_sw_wslices(const int32_t* __restrict__ wcnt, int32_t nwin, int32_t* __restrict__ wsl) {
@@ -310,15 +318,31 @@ __device__ __forceinline__ void sw_warp(const uint16_t* __restrict__ col, const 
                     v[i] = vn[i];
                 }
             }
-            // the batch in registers, then the tail
+            // the batch in registers, with the tail's loads (fewer than
+            // kSwUnroll steps) issued first as one predicated batch
+            const int kt = k + kSwUnroll;
+            uint32_t ct[kSwUnroll];
+            T vt[kSwUnroll];
+#pragma unroll
+            for (int i = 0; i < kSwUnroll; ++i) {
+                ct[i] = 0;
+                vt[i] = T(0);
+                if (kt + i < L) {
+                    ct[i] = __ldcs(cp + 32 * (kt + i));
+                    vt[i] = sw_ld<T>(vp + 32 * (kt + i));
+                }
+            }
 #pragma unroll
             for (int i = 0; i < kSwUnroll; ++i) {
                 const T p = prod(c[i], v[i]);
                 if (k + i < ln) acc = S::add(acc, p);
             }
-            for (k += kSwUnroll; k < L; ++k) {
-                const T p = prod(__ldcs(cp + 32 * k), sw_ld<T>(vp + 32 * k));
-                if (k < ln) acc = S::add(acc, p);
+#pragma unroll
+            for (int i = 0; i < kSwUnroll; ++i) {
+                if (kt + i < L) {
+                    const T p = prod(ct[i], vt[i]);
+                    if (kt + i < ln) acc = S::add(acc, p);
+                }
             }
             sw_emit<SR, T>(out, r, ln, acc, nrows, bad_row);
         } else {
@@ -339,23 +363,25 @@ __device__ __forceinline__ void sw_warp(const uint16_t* __restrict__ col, const 
                     v[t] = sw_ld<T>(vp + 32 * t);
                 }
             }
+            const bool unit = steps == m;  // every slice one step long (the common case)
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 r[j] = -1;
                 ln[j] = 0;
                 if (j < m) {
                     r[j] = __ldg(prow + (int64_t)(it.y + j) * 32 + lane);
-                    ln[j] = __ldg(plen + (int64_t)(it.y + j) * 32 + lane);
+                    // a one-step slice's lane holds one entry or none (row -1)
+                    if (!unit) ln[j] = __ldg(plen + (int64_t)(it.y + j) * 32 + lane);
                 }
             }
             T p[8];
 #pragma unroll
             for (int t = 0; t < 8; ++t) p[t] = t < steps ? prod(c[t], v[t]) : S::identity();
-            if (steps == m) {
-                // every slice one step long (the common case): lane's piece j is entry j
+            if (unit) {
+                // lane's piece j is entry j
 #pragma unroll
                 for (int j = 0; j < 8; ++j)
-                    if (j < m) sw_emit<SR, T>(out, r[j], ln[j], p[j], nrows, bad_row);
+                    if (j < m) sw_emit<SR, T>(out, r[j], r[j] >= 0 ? 1 : 0, p[j], nrows, bad_row);
             } else {
                 int base = 0;
 #pragma unroll
@@ -592,10 +618,13 @@ void sw_cut_shares(const std::vector<double>& acc, int nsh, std::vector<int32_t>
 }
 
 // Calibrated shares: time every CTA's share (plus-times over x = 1, SM
-// cycles), spread each share's time over its items by the modelled cost and
-// cut again at equal time; a few rounds settle it (the model alone leaves
-// CTAs idle for half of a launch on power-law graphs).
-constexpr int kSwCalibrationRounds = 10;
+// cycles, the median of three warm launches), spread each share's time over
+// its items by the modelled cost, average with the previous rounds' estimate
+// and cut again at equal time; the shares whose slowest CTA was fastest over
+// all rounds are kept (the model alone leaves CTAs idle for half of a launch
+// on power-law graphs, and a single round's cut moves with timing noise).
+constexpr int kSwCalibrationRounds = 12;
+constexpr int kSwCalibrationReps = 3;
 
 template <typename T>
 __global__ void k_sw_fill_one(T* v, int64_t n) {
@@ -613,14 +642,32 @@ int sw_calibrate(SellW* f, const std::vector<double>& cost, std::vector<int32_t>
     k_sw_fill_one<float><<<sw_blocks(f->ncols), 256, 0, s>>>(x1, f->ncols);
     GBK_LAUNCHED();
     std::vector<long long> t(nsh);
-    std::vector<double> w(ni + 1);
+    std::vector<std::vector<long long>> reps(kSwCalibrationReps, std::vector<long long>(nsh));
+    std::vector<double> w(ni + 1), wavg;
+    std::vector<int32_t> best = share;
+    long long best_max = -1;
     int rc = GBK_SUCCESS;
     for (int round = 0; round < kSwCalibrationRounds && rc == GBK_SUCCESS; ++round) {
-        for (int rep = 0; rep < 2 && rc == GBK_SUCCESS; ++rep)  // the second launch is timed warm
+        rc = launch_sellw<GBK_PLUS_TIMES, float>(f, x1, (float*)f->tmp, false, s, clk);  // warm-up
+        for (int rep = 0; rep < kSwCalibrationReps && rc == GBK_SUCCESS; ++rep) {
             rc = launch_sellw<GBK_PLUS_TIMES, float>(f, x1, (float*)f->tmp, false, s, clk);
+            if (rc != GBK_SUCCESS) break;
+            GBK_CUDA(cudaMemcpyAsync(reps[rep].data(), clk, sizeof(long long) * nsh, cudaMemcpyDeviceToHost, s));
+        }
         if (rc != GBK_SUCCESS) break;
-        GBK_CUDA(cudaMemcpyAsync(t.data(), clk, sizeof(long long) * nsh, cudaMemcpyDeviceToHost, s));
         GBK_CUDA(cudaStreamSynchronize(s));
+        long long tmax = 0;
+        for (int b = 0; b < nsh; ++b) {
+            long long v[kSwCalibrationReps];
+            for (int r = 0; r < kSwCalibrationReps; ++r) v[r] = reps[r][b];
+            std::sort(v, v + kSwCalibrationReps);
+            t[b] = v[kSwCalibrationReps / 2];
+            tmax = std::max(tmax, t[b]);
+        }
+        if (best_max < 0 || tmax < best_max) {
+            best_max = tmax;
+            best = share;
+        }
         double tsum = 0, csum = 0;
         for (int b = 0; b < nsh; ++b)
             if (share[b + 1] > share[b] && t[b] > 0) {
@@ -638,9 +685,16 @@ int sw_calibrate(SellW* f, const std::vector<double>& cost, std::vector<int32_t>
             for (int64_t q = q0 + 1; q <= q1; ++q) w[q] = acc + tb * (cost[q] - cost[q0]) / cb;
             acc += tb;
         }
-        sw_cut_shares(w, nsh, share);
+        if (wavg.empty()) {
+            wavg = w;
+        } else {
+            for (int64_t q = 0; q <= ni; ++q) wavg[q] = 0.5 * (wavg[q] + w[q]);
+        }
+        sw_cut_shares(wavg, nsh, share);
         GBK_CUDA(cudaMemcpyAsync(f->share, share.data(), 4 * share.size(), cudaMemcpyHostToDevice, s));
     }
+    share = best;
+    GBK_CUDA(cudaMemcpyAsync(f->share, share.data(), 4 * share.size(), cudaMemcpyHostToDevice, s));
     GBK_CUDA(cudaStreamSynchronize(s));
     cudaFree(x1);
     cudaFree(clk);
@@ -692,7 +746,7 @@ int build_impl(const CsrView& a0, bool reorder, SellW** out, cudaStream_t s) {
     GBK_CUDA(cudaMalloc(&pflag, 4 * (nnz + 1)));
     GBK_CUDA(cudaMalloc(&pid, 4 * (nnz + 1)));
     // entries by (window, row), in CSR order inside each
-    k_sw_keys<<<sw_blocks(a.nrows), 256, 0, s>>>(a.ptr, a.idx, a.nrows, keys, pos);
+    k_sw_keys<<<sw_blocks(nnz), 256, 0, s>>>(a.ptr, a.idx, a.nrows, nnz, keys, pos);
     GBK_LAUNCHED();
     int win_bits = 1;
     while ((1ll << win_bits) < f->nwin) ++win_bits;

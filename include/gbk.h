@@ -42,7 +42,7 @@ typedef struct gbk_format_params {
     int32_t seg_staged;      /* CSR_SEG / LAV: 0 (default) windows of 49152 columns whose x values are
                                 staged in shared memory, row sums folded into y atomically; -1 =
                                 seg_cols-wide segments gathered from L2 and merged per row in segment
-                                order.  SELL-C: 1 = SELL-C-sigma built inside staged windows of 49152
+                                order.  SELL-C: 1 = SELL-C-sigma built inside staged windows of 45056
                                 columns (sigma = the window, virtual rows in pieces of at most 32 entries;
                                 sell_reorder_cols renumbers the columns by in-degree first); 0 (default)
                                 = the gathered SELL-C */
