@@ -6,6 +6,8 @@
 // atomic fetch-add cursors, which leaves rows in arbitrary order inside a
 // column; here the CSC is produced by a radix sort on (col, row) keys, so
 // rows are ascending within each column and every run is deterministic.
+#include <algorithm>
+
 #include <cub/cub.cuh>
 
 #include "common.cuh"
@@ -115,20 +117,25 @@ int ensure_csc(gbk_matrix A, cudaStream_t s) {
     GBK_CUDA(cudaMalloc(&t.val, eb * (nnz > 0 ? nnz : 1)));
     GBK_CUDA(cudaMemsetAsync(t.ptr, 0, sizeof(int32_t) * (t.nrows + 1), s));
     if (nnz > 0) {
+        // temporaries from the stream-ordered pool (no device-wide
+        // synchronisation per allocation or free)
         unsigned long long *keys = nullptr, *keys2 = nullptr;
         int32_t *pos = nullptr, *pos2 = nullptr;
-        GBK_CUDA(cudaMalloc(&keys, sizeof(unsigned long long) * nnz));
-        GBK_CUDA(cudaMalloc(&keys2, sizeof(unsigned long long) * nnz));
-        GBK_CUDA(cudaMalloc(&pos, sizeof(int32_t) * nnz));
-        GBK_CUDA(cudaMalloc(&pos2, sizeof(int32_t) * nnz));
+        GBK_CUDA(cudaMallocAsync(&keys, sizeof(unsigned long long) * nnz, s));
+        GBK_CUDA(cudaMallocAsync(&keys2, sizeof(unsigned long long) * nnz, s));
+        GBK_CUDA(cudaMallocAsync(&pos, sizeof(int32_t) * nnz, s));
+        GBK_CUDA(cudaMallocAsync(&pos2, sizeof(int32_t) * nnz, s));
         k_transpose_keys<<<(unsigned)((nnz + 255) / 256), 256, 0, s>>>(a.ptr, a.idx, a.nrows, nnz, keys, pos);
         GBK_LAUNCHED();
+        // The entries come in row order, so a stable sort on the column bits
+        // alone leaves each column's rows ascending: the low 32 bits (the
+        // row) need no passes of their own.
         size_t tmp_bytes = 0;
         const int end_bit = 32 + bits_for(a.ncols + 1);
-        cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys2, pos, pos2, (int)nnz, 0, end_bit, s);
+        cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys2, pos, pos2, (int)nnz, 32, end_bit, s);
         void* tmp = nullptr;
-        GBK_CUDA(cudaMalloc(&tmp, tmp_bytes));
-        GBK_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys2, pos, pos2, (int)nnz, 0, end_bit, s));
+        GBK_CUDA(cudaMallocAsync(&tmp, std::max<size_t>(tmp_bytes, 16), s));
+        GBK_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys2, pos, pos2, (int)nnz, 32, end_bit, s));
         count_launch(1);
         // column counts land in ptr[1..], then an inclusive scan gives ptr
         k_transpose_finish<<<(unsigned)((nnz + 255) / 256), 256, 0, s>>>(
@@ -137,16 +144,11 @@ int ensure_csc(gbk_matrix A, cudaStream_t s) {
         size_t scan_bytes = 0;
         cub::DeviceScan::InclusiveSum(nullptr, scan_bytes, t.ptr + 1, t.ptr + 1, (int)t.nrows, s);
         void* scan_tmp = nullptr;
-        GBK_CUDA(cudaMalloc(&scan_tmp, scan_bytes));
+        GBK_CUDA(cudaMallocAsync(&scan_tmp, std::max<size_t>(scan_bytes, 16), s));
         GBK_CUDA(cub::DeviceScan::InclusiveSum(scan_tmp, scan_bytes, t.ptr + 1, t.ptr + 1, (int)t.nrows, s));
         count_launch(1);
+        for (void* p : {scan_tmp, tmp, (void*)keys, (void*)keys2, (void*)pos, (void*)pos2}) cudaFreeAsync(p, s);
         GBK_CUDA(cudaStreamSynchronize(s));
-        cudaFree(scan_tmp);
-        cudaFree(tmp);
-        cudaFree(keys);
-        cudaFree(keys2);
-        cudaFree(pos);
-        cudaFree(pos2);
     }
     int rc = build_tiles(t, (int)eb, s);
     if (rc) return rc;

@@ -47,6 +47,7 @@
 // search for each lane's row), longer rows are cut into kChunk-entry chunks
 // that a second kernel of the same level hands out one per warp.
 #include <algorithm>
+#include <cstdlib>
 
 #include "common.cuh"
 #include "internal.h"
@@ -104,9 +105,25 @@ int build_loop_graph(cudaGraph_t* graph, cudaGraphExec_t* exec, Body body) {
 }
 
 // Launches the loop graph once on s and releases it (an executable graph
-// destroyed while it runs is released when it ends).
+// destroyed while it runs is released when it ends).  With GBK_HOST_LOOP=1
+// (or GBK_BATCH_HOST_LOOP=1) in the environment -- for profilers that do not
+// follow conditional graph nodes -- the same body kernels are launched from a
+// host loop instead, one round trip per iteration, until the control kernel
+// clears *d_cont.
 template <typename Body>
-int run_loop_graph(cudaStream_t s, Body body) {
+int run_loop_graph(cudaStream_t s, const int32_t* d_cont, Body body) {
+    const char* e1 = getenv("GBK_HOST_LOOP");
+    const char* e2 = getenv("GBK_BATCH_HOST_LOOP");
+    if ((e1 && e1[0] == '1') || (e2 && e2[0] == '1')) {
+        for (;;) {
+            body(s, (cudaGraphConditionalHandle)0);
+            GBK_CUDA(cudaGetLastError());
+            int32_t cont = 0;
+            GBK_CUDA(cudaMemcpyAsync(&cont, d_cont, 4, cudaMemcpyDeviceToHost, s));
+            GBK_CUDA(cudaStreamSynchronize(s));
+            if (!cont) return GBK_SUCCESS;
+        }
+    }
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int rc = build_loop_graph(&graph, &exec, body);
@@ -224,6 +241,7 @@ struct Bfs1State {
     int32_t max_level;
     int32_t direction;    // 0 switch by the rule above, 1 top-down only, 2 bottom-up only
     int32_t nchunks;      // heavy-row chunks appended this level
+    int32_t cont;         // another level runs
 };
 
 struct Bfs1Bufs {
@@ -361,7 +379,8 @@ __global__ void k_bfs1_control(Bfs1State* st, int64_t n, cudaGraphConditionalHan
     st->ncount = 0;
     st->nedges = 0;
     st->nchunks = 0;
-    cudaGraphSetConditional(h, cont ? 1u : 0u);
+    st->cont = cont ? 1 : 0;
+    if (h) cudaGraphSetConditional(h, cont ? 1u : 0u);
 }
 
 __global__ void k_bfs1_init(Bfs1Bufs b, Bfs1State* st, int32_t src, long long nnz, int alpha, int beta,
@@ -426,6 +445,7 @@ struct Sssp1State {
     T thr_prev;          // the threshold before the running split
     T delta;
     T far_min;           // smallest distance kept in the pile by the running split
+    int32_t cont;        // another round runs
 };
 
 template <typename T>
@@ -579,7 +599,8 @@ __global__ void k_sssp1_control(Sssp1State<T>* st, cudaGraphConditionalHandle h)
     if (cont) st->round += 1;
     st->ncount = 0;
     st->nchunks = 0;
-    cudaGraphSetConditional(h, cont ? 1u : 0u);
+    st->cont = cont ? 1 : 0;
+    if (h) cudaGraphSetConditional(h, cont ? 1u : 0u);
 }
 
 template <typename T>
@@ -683,7 +704,7 @@ int run_sssp1(gbk_matrix A, int32_t source, double delta, T* dist, int32_t* roun
         count_launch(1);
     }
     if (rc == GBK_SUCCESS)
-        rc = run_loop_graph(s, [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
+        rc = run_loop_graph(s, &st->cont, [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
             k_sssp1_light<T><<<grid, kT, 0, cs>>>(b, st);
             k_sssp1_heavy<T><<<grid, kT, 0, cs>>>(b, st);
             k_sssp1_control<T><<<1, 32, 0, cs>>>(st, h);
@@ -1022,7 +1043,7 @@ extern "C" int gbk_bfs_levels(gbk_matrix A, int64_t source, int direction, gbk_d
     rc = e == cudaSuccess ? GBK_SUCCESS : cuda_fail(e, "k_bfs1_init", __FILE__, __LINE__);
     count_launch(1);
     if (rc == GBK_SUCCESS)
-        rc = run_loop_graph(s, [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
+        rc = run_loop_graph(s, &st->cont, [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
             k_bfs1_light<<<grid, kT, 0, cs>>>(b, st);
             k_bfs1_heavy<<<grid, kT, 0, cs>>>(b, st);
             k_bfs1_control<<<1, 32, 0, cs>>>(st, b.n, h);
@@ -1154,7 +1175,7 @@ extern "C" int gbk_pagerank(gbk_matrix A, int32_t itermax, double damping, doubl
     }
     if (rc == GBK_SUCCESS && h.cont) {
         int irc = GBK_SUCCESS;
-        rc = run_loop_graph(s, [&](cudaStream_t cs, cudaGraphConditionalHandle hd) { irc = iterate(cs, hd); });
+        rc = run_loop_graph(s, &st->cont, [&](cudaStream_t cs, cudaGraphConditionalHandle hd) { irc = iterate(cs, hd); });
         if (rc == GBK_SUCCESS) rc = irc;
         if (rc == GBK_SUCCESS) {
             fail(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s), "gbk_pagerank state");

@@ -956,11 +956,12 @@ int build_segmented(const CsrView& a, const std::vector<int32_t>& col_seg_h, con
         GBK_CUDA(cudaMalloc(&vid, 4 * (nnz + 1)));
         k_seg_keys<<<blocks_for(nnz), 256, 0, s>>>(a.ptr, a.idx, n, nnz, col_seg, keys, pos);
         GBK_LAUNCHED();
+        // entries in row order: a stable sort on the segment bits suffices
         size_t tb = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, pos, pos2, (int)nnz, 0, 64, s);
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, pos, pos2, (int)nnz, 32, 64, s);
         void* tmp = nullptr;
         GBK_CUDA(cudaMalloc(&tmp, tb));
-        GBK_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, pos, pos2, (int)nnz, 0, 64, s));
+        GBK_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, pos, pos2, (int)nnz, 32, 64, s));
         count_launch(1);
         GBK_CUDA(cudaMemsetAsync(flag + nnz, 0, 4, s));
         k_vrow_flags<<<blocks_for(nnz), 256, 0, s>>>(keys2, nnz, flag);

@@ -638,10 +638,10 @@ int build_impl(const CsrView& a, SegSmem** out, cudaStream_t s) {
         int seg_bits = 1;
         while ((1ll << seg_bits) < f->nseg) ++seg_bits;
         size_t tb = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, pos, pos2, (int)nnz, 0, 32 + seg_bits, s);
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, pos, pos2, (int)nnz, 32, 32 + seg_bits, s);
         void* tmp = nullptr;
         GBK_CUDA(cudaMalloc(&tmp, std::max<size_t>(tb, 16)));
-        GBK_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, pos, pos2, (int)nnz, 0, 32 + seg_bits, s));
+        GBK_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, pos, pos2, (int)nnz, 32, 32 + seg_bits, s));
         count_launch(1);
         GBK_CUDA(cudaMemsetAsync(f->seg_start, 0xff, 4 * (f->nseg + 1), s));
         GBK_CUDA(cudaMemsetAsync(flag + nnz, 0, 4, s));

@@ -737,35 +737,36 @@ int build_impl(const CsrView& a0, bool reorder, SellW** out, cudaStream_t s) {
     }
     unsigned long long *keys = nullptr, *keys2 = nullptr;
     int32_t *pos = nullptr, *pos2 = nullptr, *vs = nullptr, *vstart = nullptr, *pflag = nullptr, *pid = nullptr;
-    GBK_CUDA(cudaMalloc(&keys, 8 * nnz));
-    GBK_CUDA(cudaMalloc(&keys2, 8 * nnz));
-    GBK_CUDA(cudaMalloc(&pos, 4 * nnz));
-    GBK_CUDA(cudaMalloc(&pos2, 4 * nnz));
-    GBK_CUDA(cudaMalloc(&vs, 4 * nnz));
-    GBK_CUDA(cudaMalloc(&vstart, 4 * nnz));
-    GBK_CUDA(cudaMalloc(&pflag, 4 * (nnz + 1)));
-    GBK_CUDA(cudaMalloc(&pid, 4 * (nnz + 1)));
-    // entries by (window, row), in CSR order inside each
+    GBK_CUDA(cudaMallocAsync(&keys, 8 * nnz, s));
+    GBK_CUDA(cudaMallocAsync(&keys2, 8 * nnz, s));
+    GBK_CUDA(cudaMallocAsync(&pos, 4 * nnz, s));
+    GBK_CUDA(cudaMallocAsync(&pos2, 4 * nnz, s));
+    GBK_CUDA(cudaMallocAsync(&vs, 4 * nnz, s));
+    GBK_CUDA(cudaMallocAsync(&vstart, 4 * nnz, s));
+    GBK_CUDA(cudaMallocAsync(&pflag, 4 * (nnz + 1), s));
+    GBK_CUDA(cudaMallocAsync(&pid, 4 * (nnz + 1), s));
+    // entries by (window, row), in CSR order inside each: the entries come
+    // in row order, so a stable sort on the window bits alone is enough
     k_sw_keys<<<sw_blocks(nnz), 256, 0, s>>>(a.ptr, a.idx, a.nrows, nnz, keys, pos);
     GBK_LAUNCHED();
     int win_bits = 1;
     while ((1ll << win_bits) < f->nwin) ++win_bits;
     size_t tb = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, pos, pos2, (int)nnz, 0, 32 + win_bits, s);
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, pos, pos2, (int)nnz, 32, 32 + win_bits, s);
     void* tmp = nullptr;
-    GBK_CUDA(cudaMalloc(&tmp, std::max<size_t>(tb, 16)));
-    GBK_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, pos, pos2, (int)nnz, 0, 32 + win_bits, s));
+    GBK_CUDA(cudaMallocAsync(&tmp, std::max<size_t>(tb, 16), s));
+    GBK_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, pos, pos2, (int)nnz, 32, 32 + win_bits, s));
     count_launch(1);
-    cudaFree(tmp);
+    cudaFreeAsync(tmp, s);
     // pieces: kSwPiece-entry parts of the virtual rows
     k_sw_vstart<<<sw_blocks(nnz), 256, 0, s>>>(keys2, nnz, vs);
     GBK_LAUNCHED();
     size_t mb = 0;
     cub::DeviceScan::InclusiveScan(nullptr, mb, vs, vstart, ::cuda::maximum<int32_t>{}, (int)nnz, s);
-    GBK_CUDA(cudaMalloc(&tmp, std::max<size_t>(mb, 16)));
+    GBK_CUDA(cudaMallocAsync(&tmp, std::max<size_t>(mb, 16), s));
     GBK_CUDA(cub::DeviceScan::InclusiveScan(tmp, mb, vs, vstart, ::cuda::maximum<int32_t>{}, (int)nnz, s));
     count_launch(1);
-    cudaFree(tmp);
+    cudaFreeAsync(tmp, s);
     k_sw_pflag<<<sw_blocks(nnz + 1), 256, 0, s>>>(vstart, nnz, pflag);
     GBK_LAUNCHED();
     GBK_CUDA(cudaStreamSynchronize(s));
@@ -779,16 +780,16 @@ int build_impl(const CsrView& a0, bool reorder, SellW** out, cudaStream_t s) {
     int32_t *pfirst = nullptr, *pidx = nullptr, *pidx2 = nullptr, *wcnt = nullptr, *wpfirst = nullptr,
             *wsl = nullptr, *slen = nullptr, *pslot = nullptr, *win_slice = nullptr;
     uint32_t *pkey = nullptr, *pkey2 = nullptr;
-    GBK_CUDA(cudaMalloc(&pfirst, 4 * (np + 1)));
-    GBK_CUDA(cudaMalloc(&pkey, 4 * np));
-    GBK_CUDA(cudaMalloc(&pkey2, 4 * np));
-    GBK_CUDA(cudaMalloc(&pidx, 4 * np));
-    GBK_CUDA(cudaMalloc(&pidx2, 4 * np));
-    GBK_CUDA(cudaMalloc(&pslot, 4 * np));
-    GBK_CUDA(cudaMalloc(&wcnt, 4 * (f->nwin + 1)));
-    GBK_CUDA(cudaMalloc(&wpfirst, 4 * (f->nwin + 1)));
-    GBK_CUDA(cudaMalloc(&wsl, 4 * (f->nwin + 1)));
-    GBK_CUDA(cudaMalloc(&win_slice, 4 * (f->nwin + 1)));
+    GBK_CUDA(cudaMallocAsync(&pfirst, 4 * (np + 1), s));
+    GBK_CUDA(cudaMallocAsync(&pkey, 4 * np, s));
+    GBK_CUDA(cudaMallocAsync(&pkey2, 4 * np, s));
+    GBK_CUDA(cudaMallocAsync(&pidx, 4 * np, s));
+    GBK_CUDA(cudaMallocAsync(&pidx2, 4 * np, s));
+    GBK_CUDA(cudaMallocAsync(&pslot, 4 * np, s));
+    GBK_CUDA(cudaMallocAsync(&wcnt, 4 * (f->nwin + 1), s));
+    GBK_CUDA(cudaMallocAsync(&wpfirst, 4 * (f->nwin + 1), s));
+    GBK_CUDA(cudaMallocAsync(&wsl, 4 * (f->nwin + 1), s));
+    GBK_CUDA(cudaMallocAsync(&win_slice, 4 * (f->nwin + 1), s));
     GBK_CUDA(cudaMemsetAsync(wcnt, 0, 4 * (f->nwin + 1), s));
     k_sw_pfirst<<<sw_blocks(nnz), 256, 0, s>>>(pflag, pid, nnz, pfirst);
     GBK_LAUNCHED();
@@ -799,10 +800,10 @@ int build_impl(const CsrView& a0, bool reorder, SellW** out, cudaStream_t s) {
     // pieces by window, then length descending (stable: row order for ties)
     tb = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, tb, pkey, pkey2, pidx, pidx2, (int)np, 0, 9 + win_bits, s);
-    GBK_CUDA(cudaMalloc(&tmp, std::max<size_t>(tb, 16)));
+    GBK_CUDA(cudaMallocAsync(&tmp, std::max<size_t>(tb, 16), s));
     GBK_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, pkey, pkey2, pidx, pidx2, (int)np, 0, 9 + win_bits, s));
     count_launch(1);
-    cudaFree(tmp);
+    cudaFreeAsync(tmp, s);
     k_sw_wcount<<<sw_blocks(np), 256, 0, s>>>(pkey2, np, wcnt);
     GBK_LAUNCHED();
     rc = sw_scan_excl(wcnt, wpfirst, f->nwin + 1, s);
@@ -818,26 +819,26 @@ int build_impl(const CsrView& a0, bool reorder, SellW** out, cudaStream_t s) {
     f->nslices = ns;
     GBK_CUDA(cudaMalloc(&f->prow, 4 * 32 * ns));
     GBK_CUDA(cudaMalloc(&f->plen, 2 * 32 * ns));
-    GBK_CUDA(cudaMalloc(&slen, 4 * (ns + 1)));
+    GBK_CUDA(cudaMallocAsync(&slen, 4 * (ns + 1), s));
     GBK_CUDA(cudaMemsetAsync(f->prow, 0xff, 4 * 32 * ns, s));
     GBK_CUDA(cudaMemsetAsync(f->plen, 0, 2 * 32 * ns, s));
     k_sw_place<<<sw_blocks(np), 256, 0, s>>>(pkey2, pidx2, np, wpfirst, win_slice, pfirst, keys2, f->prow, f->plen,
                                              slen, pslot);
     GBK_LAUNCHED();
     long long *ent = nullptr, *soff = nullptr;
-    GBK_CUDA(cudaMalloc(&ent, 8 * (ns + 1)));
-    GBK_CUDA(cudaMalloc(&soff, 8 * (ns + 1)));
+    GBK_CUDA(cudaMallocAsync(&ent, 8 * (ns + 1), s));
+    GBK_CUDA(cudaMallocAsync(&soff, 8 * (ns + 1), s));
     k_sw_steps<<<sw_blocks(ns + 1), 256, 0, s>>>(slen, ns, ent);
     GBK_LAUNCHED();
     size_t eb = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, eb, ent, soff, (int)(ns + 1), s);
-    GBK_CUDA(cudaMalloc(&tmp, std::max<size_t>(eb, 16)));
+    GBK_CUDA(cudaMallocAsync(&tmp, std::max<size_t>(eb, 16), s));
     GBK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, eb, ent, soff, (int)(ns + 1), s));
     count_launch(1);
     long long padded = 0;
     GBK_CUDA(cudaMemcpyAsync(&padded, soff + ns, 8, cudaMemcpyDeviceToHost, s));
     GBK_CUDA(cudaStreamSynchronize(s));
-    cudaFree(tmp);
+    cudaFreeAsync(tmp, s);
     if (padded >= (1ll << 31)) {
         set_error("staged SELL-C: %lld padded entries exceed 2^31", padded);
         return fail(GBK_INSUFFICIENT_SPACE);
@@ -871,9 +872,9 @@ int build_impl(const CsrView& a0, bool reorder, SellW** out, cudaStream_t s) {
     GBK_CUDA(cudaStreamSynchronize(s));
     for (void* p : {(void*)keys, (void*)keys2, (void*)pos, (void*)pos2, (void*)vs, (void*)vstart, (void*)pflag,
                     (void*)pid, (void*)pfirst, (void*)pkey, (void*)pkey2, (void*)pidx, (void*)pidx2, (void*)pslot,
-                    (void*)wcnt, (void*)wpfirst, (void*)wsl, (void*)slen, (void*)ent, (void*)soff, (void*)idx2,
-                    (void*)win_slice})
-        cudaFree(p);
+                    (void*)wcnt, (void*)wpfirst, (void*)wsl, (void*)slen, (void*)ent, (void*)soff, (void*)win_slice})
+        cudaFreeAsync(p, s);  // build temporaries come from the stream-ordered pool
+    cudaFree(idx2);
     if (std::is_same<T, float>::value && f->nitems > 0) {
         rc = sw_calibrate(f, cost, share, s);
         if (rc != GBK_SUCCESS) return fail(rc);
