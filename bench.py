@@ -69,10 +69,13 @@ def parse():
     p.add_argument("--seed", type=int, default=42)
     p.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--mode", default="spmv", choices=["spmv", "batched", "serve", "algorithms", "ingest", "spgemm"],
+    p.add_argument("--mode", default="spmv",
+                   choices=["spmv", "batched", "serve", "algorithms", "single", "ingest", "spgemm"],
                    help="spmv: the SpMV line (default); batched: 64-source BFS + 32-column PPR / SSSP on "
                         "R-MAT s22; serve: Poisson request stream on a resident undirected R-MAT s24; "
                         "algorithms: BFS/CC/PR/SSSP/TC on undirected R-MAT s23 vs the reference CPU code; "
+                        "single: the device-loop BFS/SSSP/CC/PageRank calls on undirected R-MAT (--alg-scale), "
+                        "--steps sources; "
                         "ingest: the R-MAT graph as .mtx / .mtxbin files into device CSR vs the reference reader; "
                         "spgemm: unmasked A*A and triangle counting on undirected R-MAT vs the reference")
     p.add_argument("--queries", type=int, default=1000, help="serve: requests in the trace")
@@ -713,6 +716,12 @@ def run_serve(args):
         res, wall = srv.run_trace(arr, kinds, srcs)
     launches = capi.launch_count() - l0
     burst, wall_b = srv.run_trace(np.zeros(nq), kinds, srcs)
+    # below capacity: the same mix at 60 % of the burst capacity, so the
+    # latencies are service times rather than queueing
+    sub_rate = 0.6 * nq / wall_b
+    sub_n = min(nq, max(100, int(sub_rate * 2.0)))
+    sa, sk, ss = poisson_trace(sub_n, sub_rate, mix=(0.5, 0.25, 0.25), candidates=cand, seed=args.seed + 8)
+    sub, sub_wall = srv.run_trace(sa, sk, ss)
     # capacity per query kind (a burst of one kind only)
     per_kind = {}
     for k, name in ((0, "bfs"), (1, "ppr"), (2, "sssp")):
@@ -762,6 +771,8 @@ def run_serve(args):
                             "uniform over non-isolated vertices", "iters_per_launch": 4,
                    "l2": "graph and batch state larger than L2"},
         "latency_ms": lat, "qps_offered": args.rate, "qps_capacity_burst": round(cap, 2),
+        "below_capacity": {"qps_offered": round(sub_rate, 2), "queries": int(sub_n),
+                           "qps": round(sub_n / sub_wall, 2), "latency_ms": latency_stats(sub)},
         "qps_capacity_per_kind": per_kind,
         "batches": nb, "device_bytes_used": used, "memory_budget": budget,
         "one_at_a_time": {"qps_poisson": round(m / wall1, 2), "qps_capacity": round(cap1, 2),
@@ -798,6 +809,9 @@ def extras_summary(args):
         o = v["one_at_a_time"]
         res["served"] = {"workload": v["config"]["workload"], "qps": v["value"], "p50_ms": v["latency_ms"]["p50_ms"],
                          "p99_ms": v["latency_ms"]["p99_ms"], "qps_capacity": v["qps_capacity_burst"],
+                         "below_capacity": {"qps_offered": v["below_capacity"]["qps_offered"],
+                                            "p50_ms": v["below_capacity"]["latency_ms"]["p50_ms"],
+                                            "p99_ms": v["below_capacity"]["latency_ms"]["p99_ms"]},
                          "qps_capacity_per_kind": v["qps_capacity_per_kind"],
                          "one_at_a_time_qps_same_engine": o["qps_capacity"],
                          "one_at_a_time_qps_best_single_query_path": o["qps_capacity_best_single_query_path"],
@@ -815,6 +829,74 @@ def extras_summary(args):
     except Exception as e:
         res["algorithms"] = {"error": str(e)[:300]}
     return res
+
+
+def run_single(args):
+    """Single-query loops on the device (gbk_bfs_levels, gbk_sssp_dist, gbk_cc_labels,
+    gbk_pagerank) on undirected R-MAT, CUDA events around each call; a few
+    sources each, the levels / distances / labels checked against the oracle."""
+    import torch
+    from gb_kun_b200 import capi, graphgen as gg
+    from oracle.cpu import Oracle
+    capi.init(0)
+    g = gg.rmat(args.alg_scale, args.edge_factor, seed=args.seed, undirected=True)
+    w = gg.weights_i32(g, seed=args.seed + 3)
+    A = capi.Matrix.from_graph(g)
+    Aw = capi.Matrix.from_graph(g, w)
+    src = [int(s) for s in gg.sources(g, max(1, args.steps), seed=args.seed + 4)]
+    deg = np.diff(g.row_ptr)
+    lv = torch.zeros(g.n, dtype=torch.int32, device="cuda")
+    dist = torch.zeros(g.n, dtype=torch.int32, device="cuda")
+    lab = torch.zeros(g.n, dtype=torch.int32, device="cuda")
+    rk = torch.zeros(g.n, device="cuda")
+    A.autotune(reps=10, semiring="plus_second")
+    for _ in range(max(1, args.warmup)):  # lazy CSC, format and degree builds
+        A.bfs(src[0], lv)
+        Aw.sssp(src[0], dist)
+        A.cc(lab)
+        A.pagerank(rk, itermax=100, damping=0.85, tol=1e-6)
+    torch.cuda.synchronize()
+
+    def ev(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), r
+
+    l0 = capi.launch_count()
+    bfs = [ev(lambda: A.bfs(s, lv)) for s in src]
+    edges = int(deg[lv.cpu().numpy() > 0].sum())
+    sssp = [ev(lambda: Aw.sssp(s, dist)) for s in src]
+    cc_ms, _ = ev(lambda: A.cc(lab))
+    pr_ms, (pr_it, _) = ev(lambda: A.pagerank(rk, itermax=100, damping=0.85, tol=1e-6))
+    launches = capi.launch_count() - l0
+    O = Oracle()
+    d64 = O.sssp(g, w, src[-1])
+    checks = {"bfs": bool(np.array_equal(lv.cpu().numpy(), O.bfs(g, src[-1]))),
+              "sssp": bool(np.array_equal(dist.cpu().numpy(),
+                                          np.where(d64 < 0, np.iinfo(np.int32).max, d64).astype(np.int32))),
+              "cc": bool(np.array_equal(lab.cpu().numpy(), O.cc(g)))}
+    r64, _, _ = O.pagerank(g, tol=0.0, itermax=pr_it)
+    checks["pagerank_rel_l1_vs_fp64"] = float(np.abs(rk.cpu().numpy() - r64).sum() / np.abs(r64).sum())
+    bfs_ms = statistics.median(t for t, _ in bfs)
+    A.close()
+    Aw.close()
+    return {
+        "metric": "single-query loops on the device: ms per query", "value": round(edges / (bfs_ms * 1e-3) / 1e9, 3),
+        "unit": "GTEPS (BFS)", "n_gpus": 1, "steps": len(src), "warmup": max(1, args.warmup),
+        "ms_per_step": round(bfs_ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "i32 levels / i32 distances / f32 ranks", "data": "synthetic (seeded R-MAT, generated in-process)",
+        "config": {"workload": f"single_query_rmat{args.alg_scale}u", "n": g.n, "nnz": g.nnz,
+                   "graph": f"R-MAT scale {args.alg_scale}, edge factor {args.edge_factor}, undirected; int32 "
+                            "weights in [1, 255] for SSSP", "sources": f"{len(src)} seeded non-isolated vertices",
+                   "timing": "CUDA events around each call (one graph launch per query)"},
+        "bfs_ms": [round(t, 4) for t, _ in bfs], "bfs_depth": bfs[-1][1],
+        "sssp_ms": [round(t, 4) for t, _ in sssp], "sssp_rounds": sssp[-1][1],
+        "cc_ms": round(cc_ms, 4), "pagerank_ms": round(pr_ms, 4), "pagerank_iterations": pr_it,
+        "gpu_launches": int(launches), "checked_against_oracle": checks,
+    }
 
 
 def run_algorithms(args, light=False):
@@ -1134,7 +1216,7 @@ def run_reference(args):
 def main():
     args = parse()
     if args.mode != "spmv":
-        out = {"batched": run_batched, "serve": run_serve, "algorithms": run_algorithms,
+        out = {"batched": run_batched, "serve": run_serve, "algorithms": run_algorithms, "single": run_single,
                "ingest": run_ingest, "spgemm": run_spgemm}[args.mode](args)
         print(json.dumps(out), flush=True)
     elif args.impl == "reference":

@@ -39,6 +39,7 @@ struct CsrView {
 struct SellC;     // spmv_formats.cu
 struct SegCsr;    // spmv_formats.cu (CSR_SEG and LAV share one layout)
 struct SegSmem;   // spmv_segsmem.cu (CSR_SEG with x windows staged in shared memory)
+struct SingleCache;  // single.cu
 struct SellW;     // spmv_sellw.cu (SELL-C-sigma inside x windows staged in shared memory)
 struct Batch;     // batched.h
 
@@ -64,6 +65,8 @@ struct gbk_matrix_s {
     int8_t pattern_symmetric = -1;  // -1 unknown; gbk_matrix_pattern_symmetric
     int32_t* coldeg = nullptr;      // entries per column, built by the first gbk_pagerank
     int64_t coldeg_zero = 0;        // columns without entries (valid with coldeg)
+    gbk::SingleCache* single = nullptr;  // scratch and graphs of the single-query loops
+    int64_t format_gen = 0;         // bumped whenever the storage format changes
     gbk_format format = GBK_FMT_CSR;
     gbk_format_params params{};
     gbk::SellC* sell[2] = {nullptr, nullptr};
@@ -90,6 +93,7 @@ int spmv_binned(const RowBins* rb, const CsrView& v, int sr, int accum, int dtyp
                 const void* mask, int mdt, int mmode, cudaStream_t s);
 
 int ensure_csc(gbk_matrix A, cudaStream_t s);
+void free_single_cache(gbk_matrix A);
 void free_batches(gbk_matrix A);  // batched.cu
 int build_tiles(CsrView& v, int elem_bytes, cudaStream_t s);
 void free_view(CsrView& v);

@@ -209,6 +209,7 @@ int gbk_matrix_create_csr(gbk_matrix* out, int64_t nrows, int64_t ncols, int64_t
 int gbk_matrix_destroy(gbk_matrix A) {
     if (!A) return GBK_SUCCESS;
     free_batches(A);
+    free_single_cache(A);
     free_formats(A);
     free_view(A->csr);
     free_view(A->csc);

@@ -104,17 +104,74 @@ int build_loop_graph(cudaGraph_t* graph, cudaGraphExec_t* exec, Body body) {
     return GBK_SUCCESS;
 }
 
-// Launches the loop graph once on s and releases it (an executable graph
-// destroyed while it runs is released when it ends).  With GBK_HOST_LOOP=1
-// (or GBK_BATCH_HOST_LOOP=1) in the environment -- for profilers that do not
-// follow conditional graph nodes -- the same body kernels are launched from a
-// host loop instead, one round trip per iteration, until the control kernel
-// clears *d_cont.
-template <typename Body>
-int run_loop_graph(cudaStream_t s, const int32_t* d_cont, Body body) {
+bool host_loop_mode() {
     const char* e1 = getenv("GBK_HOST_LOOP");
     const char* e2 = getenv("GBK_BATCH_HOST_LOOP");
-    if ((e1 && e1[0] == '1') || (e2 && e2[0] == '1')) {
+    return (e1 && e1[0] == '1') || (e2 && e2[0] == '1');
+}
+
+}  // namespace
+
+// One loop kept per matrix: its scratch (allocated once) and its
+// instantiated graph, whose kernel arguments point into that scratch, so a
+// call only launches the init kernel and the graph (building and
+// instantiating the graph took as long as a whole BFS at R-MAT scale 23).
+struct CachedLoop {
+    void* mem = nullptr;
+    size_t bytes = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t key = -1;  // what the graph was built for (PageRank: the matrix's format generation)
+    void drop_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        key = -1;
+    }
+    void release() {
+        drop_graph();
+        cudaFree(mem);
+        mem = nullptr;
+        bytes = 0;
+    }
+};
+
+struct SingleCache {
+    CachedLoop bfs, sssp, pr;
+    double mean_weight = -1.0;  // sampled mean edge value (SSSP's automatic delta)
+};
+
+void free_single_cache(gbk_matrix A) {
+    if (!A->single) return;
+    A->single->bfs.release();
+    A->single->sssp.release();
+    A->single->pr.release();
+    delete A->single;
+    A->single = nullptr;
+}
+
+namespace {
+
+SingleCache& single_cache(gbk_matrix A) {
+    if (!A->single) A->single = new SingleCache();
+    return *A->single;
+}
+
+// The loop's scratch: allocated on first use (or grown), then kept.
+int loop_scratch(CachedLoop& L, size_t bytes) {
+    if (L.mem && L.bytes >= bytes) return GBK_SUCCESS;
+    L.release();
+    GBK_CUDA(cudaMalloc(&L.mem, bytes));
+    L.bytes = bytes;
+    return GBK_SUCCESS;
+}
+
+// Runs the loop on s: the cached graph (built on first use, or again when
+// `key` changed), or the host loop for profilers.
+template <typename Body>
+int launch_loop(CachedLoop& L, int64_t key, cudaStream_t s, const int32_t* d_cont, Body body) {
+    if (host_loop_mode()) {
         for (;;) {
             body(s, (cudaGraphConditionalHandle)0);
             GBK_CUDA(cudaGetLastError());
@@ -124,17 +181,18 @@ int run_loop_graph(cudaStream_t s, const int32_t* d_cont, Body body) {
             if (!cont) return GBK_SUCCESS;
         }
     }
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    int rc = build_loop_graph(&graph, &exec, body);
-    if (rc == GBK_SUCCESS) {
-        cudaError_t e = cudaGraphLaunch(exec, s);
-        if (e != cudaSuccess) rc = cuda_fail(e, "cudaGraphLaunch", __FILE__, __LINE__);
-        count_launch(1);
+    if (L.exec && L.key != key) L.drop_graph();
+    if (!L.exec) {
+        const int rc = build_loop_graph(&L.graph, &L.exec, body);
+        if (rc != GBK_SUCCESS) {
+            L.drop_graph();
+            return rc;
+        }
+        L.key = key;
     }
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    return rc;
+    GBK_CUDA(cudaGraphLaunch(L.exec, s));
+    count_launch(1);
+    return GBK_SUCCESS;
 }
 
 // ---- frontier expansion -----------------------------------------------------
@@ -652,18 +710,20 @@ __global__ void __launch_bounds__(1024) k_sample_mean(const T* __restrict__ w, i
 template <typename T>
 int run_sssp1(gbk_matrix A, int32_t source, double delta, T* dist, int32_t* rounds, cudaStream_t s) {
     const int64_t n = A->csr.nrows, nnz = A->csr.nnz;
+    SingleCache& C = single_cache(A);
+    CachedLoop& L = C.sssp;
+    const int64_t nwords = (n + 31) / 32;
+    const size_t st_b = 256, q_b = 4 * (size_t)n, bm_b = 4 * (size_t)nwords, d_b = sizeof(T) * (size_t)n,
+                 ch_b = sizeof(Chunk) * (size_t)max_chunks(nnz);
+    int rc = loop_scratch(L, st_b + ch_b + 4 * q_b + 3 * bm_b + d_b);
+    if (rc) return rc;
     Sssp1Bufs<T> b{};
     b.rp = A->csr.ptr;
     b.col = A->csr.idx;
     b.w = (const T*)A->csr.val;
     b.n = n;
-    b.nwords = (n + 31) / 32;
-    b.dist = dist;
-    void* mem = nullptr;
-    const size_t st_b = 256, q_b = 4 * (size_t)n, bm_b = 4 * (size_t)b.nwords,
-                 ch_b = sizeof(Chunk) * (size_t)max_chunks(nnz);
-    GBK_CUDA(cudaMallocAsync(&mem, st_b + ch_b + 4 * q_b + 3 * bm_b, s));
-    char* m = (char*)mem;
+    b.nwords = nwords;
+    char* m = (char*)L.mem;
     Sssp1State<T>* st = (Sssp1State<T>*)m;
     b.chunks = (Chunk*)(m + st_b);
     m += st_b + ch_b;
@@ -674,20 +734,24 @@ int run_sssp1(gbk_matrix A, int32_t source, double delta, T* dist, int32_t* roun
     b.bm[0] = (uint32_t*)(m + 4 * q_b);
     b.bm[1] = (uint32_t*)(m + 4 * q_b + bm_b);
     b.fbm = (uint32_t*)(m + 4 * q_b + 2 * bm_b);
-    int rc = GBK_SUCCESS;
+    b.dist = (T*)(m + 4 * q_b + 3 * bm_b);  // 4-byte aligned: every part above is a multiple of 4 bytes
     auto fail = [&](cudaError_t e, const char* what) {
         if (rc == GBK_SUCCESS && e != cudaSuccess) rc = cuda_fail(e, what, __FILE__, __LINE__);
     };
-    if (delta == 0.0 && nnz > 0) {
-        // 8 x mean weight / mean row length (R-MAT scale 23 with weights in
-        // [1, 255]: 10.1 ms at 8x, 10.8 ms at 32x, 11.4 ms without the pile)
+    if (delta == 0.0 && nnz > 0 && C.mean_weight < 0.0) {
         double* mean = (double*)st;  // the state is written after this
         k_sample_mean<T><<<1, 1024, 0, s>>>(b.w, nnz, mean);
         count_launch(1);
         double h = 0.0;
         fail(cudaMemcpyAsync(&h, mean, sizeof(h), cudaMemcpyDeviceToHost, s), "SSSP weight sample");
         fail(cudaStreamSynchronize(s), "SSSP weight sample");
-        delta = h > 0.0 ? 8.0 * h * (double)n / (double)nnz : -1.0;
+        C.mean_weight = h;
+    }
+    if (delta == 0.0) {
+        // 8 x mean weight / mean row length (R-MAT scale 23 with weights in
+        // [1, 255]: 10.1 ms at 8x, 10.8 ms at 32x, 11.4 ms without the pile)
+        const double h = C.mean_weight;
+        delta = nnz > 0 && h > 0.0 ? 8.0 * h * (double)n / (double)nnz : -1.0;
     }
     const bool use_far = delta > 0.0;
     T dl = T(1);
@@ -704,18 +768,18 @@ int run_sssp1(gbk_matrix A, int32_t source, double delta, T* dist, int32_t* roun
         count_launch(1);
     }
     if (rc == GBK_SUCCESS)
-        rc = run_loop_graph(s, &st->cont, [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
+        rc = launch_loop(L, 0, s, &st->cont, [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
             k_sssp1_light<T><<<grid, kT, 0, cs>>>(b, st);
             k_sssp1_heavy<T><<<grid, kT, 0, cs>>>(b, st);
             k_sssp1_control<T><<<1, 32, 0, cs>>>(st, h);
         });
+    if (rc == GBK_SUCCESS) fail(cudaMemcpyAsync(dist, b.dist, d_b, cudaMemcpyDeviceToDevice, s), "SSSP distances");
     if (rc == GBK_SUCCESS && rounds) {
         Sssp1State<T> h{};
         fail(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s), "SSSP rounds");
         fail(cudaStreamSynchronize(s), "SSSP rounds");
         *rounds = h.round;
     }
-    cudaFreeAsync(mem, s);
     return rc;
 }
 
@@ -731,6 +795,8 @@ struct PrState {
     float d_over_n;    // damping / n
     float sink;        // sum of the current ranks over the sinks
     float rdiff;       // sum |old - new| of the last iteration
+    float damping;
+    float inv_damping; // 1 / damping
 };
 
 struct PrBufs {
@@ -741,8 +807,6 @@ struct PrBufs {
     float* y;            // A w
     float* part_sink;    // per-block partial sums
     float* part_diff;
-    float damping;
-    float inv_damping;   // 1 / damping
     int64_t nsinks;      // columns without entries
     int sparse_sink;     // 1: the sink mass is the sum of the first nsinks ranks
 };
@@ -757,8 +821,8 @@ __device__ __forceinline__ bool pr_sink_term(const PrBufs& b, int64_t i, int32_t
 }
 
 // d = max(deg / damping, 1 / damping), in float as the reference computes it
-__device__ __forceinline__ float pr_d(const PrBufs& b, int32_t deg) {
-    return fmaxf((float)deg / b.damping, b.inv_damping);
+__device__ __forceinline__ float pr_d(float damping, float inv_damping, int32_t deg) {
+    return fmaxf((float)deg / damping, inv_damping);
 }
 
 template <int NT>
@@ -777,12 +841,13 @@ __device__ __forceinline__ float block_sum(float v) {
 }
 
 // r0 = 1 / n, w = r0 ./ d, partial sums of r0 over the sinks
-__global__ void __launch_bounds__(kT) k_pr_init(PrBufs b, float r0) {
+__global__ void __launch_bounds__(kT) k_pr_init(PrBufs b, const PrState* st, float r0) {
+    const float dmp = st->damping, inv = st->inv_damping;
     float sink = 0.0f;
     for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < b.n; i += (int64_t)gridDim.x * kT) {
         const int32_t dg = b.deg[i];
         b.r[0][i] = r0;
-        b.w[i] = r0 / pr_d(b, dg);
+        b.w[i] = r0 / pr_d(dmp, inv, dg);
         if (pr_sink_term(b, i, dg)) sink += r0;
     }
     sink = block_sum<kT>(sink);
@@ -797,6 +862,7 @@ __global__ void __launch_bounds__(kT) k_pr_init(PrBufs b, float r0) {
 // new ranks over the sinks; w = r_new ./ d for the next product
 __global__ void __launch_bounds__(kT) k_pr_post(PrBufs b, const PrState* st) {
     const float teleport = st->scaled + st->d_over_n * st->sink;
+    const float dmp = st->damping, inv = st->inv_damping;
     const float* __restrict__ ro = b.r[st->cur];
     float* __restrict__ rn = b.r[st->cur ^ 1];
     float sink = 0.0f, diff = 0.0f;
@@ -805,7 +871,7 @@ __global__ void __launch_bounds__(kT) k_pr_post(PrBufs b, const PrState* st) {
         const float r = teleport + b.y[i];
         diff += fabsf(ro[i] - r);
         rn[i] = r;
-        b.w[i] = r / pr_d(b, dg);
+        b.w[i] = r / pr_d(dmp, inv, dg);
         if (pr_sink_term(b, i, dg)) sink += r;
     }
     sink = block_sum<kT>(sink);
@@ -1016,6 +1082,11 @@ extern "C" int gbk_bfs_levels(gbk_matrix A, int64_t source, int direction, gbk_d
     cudaStream_t s = (cudaStream_t)stream;
     int rc = ensure_csc(A, s);
     if (rc) return rc;
+    CachedLoop& L = single_cache(A).bfs;
+    const size_t st_b = 256, lv_b = 4 * (size_t)n, q_b = 4 * (size_t)n, bm_b = 4 * (size_t)((n + 31) / 32),
+                 ch_b = sizeof(Chunk) * (size_t)max_chunks(A->csr.nnz);
+    rc = loop_scratch(L, st_b + ch_b + lv_b + 2 * q_b + 3 * bm_b);
+    if (rc) return rc;
     Bfs1Bufs b{};
     b.rp = A->csr.ptr;
     b.col = A->csr.idx;
@@ -1023,17 +1094,11 @@ extern "C" int gbk_bfs_levels(gbk_matrix A, int64_t source, int direction, gbk_d
     b.crow = A->csc.idx;
     b.n = n;
     b.nwords = (n + 31) / 32;
-    void* mem = nullptr;
-    const size_t st_b = 256, lv_b = 4 * (size_t)n, q_b = 4 * (size_t)n, bm_b = 4 * (size_t)b.nwords,
-                 ch_b = sizeof(Chunk) * (size_t)max_chunks(A->csr.nnz);
-    GBK_CUDA(cudaMallocAsync(&mem, st_b + ch_b + lv_b + 2 * q_b + 3 * bm_b, s));
-    char* m = (char*)mem;
+    char* m = (char*)L.mem;
     Bfs1State* st = (Bfs1State*)m;
     b.chunks = (Chunk*)(m + st_b);
     m += st_b + ch_b;
-    // int32 levels are written in place; other types are converted at the end
-    const bool direct = level_type == GBK_I32;
-    b.lv = direct ? (int32_t*)levels : (int32_t*)m;
+    b.lv = (int32_t*)m;
     b.q[0] = (int32_t*)(m + lv_b);
     b.q[1] = (int32_t*)(m + lv_b + q_b);
     for (int k = 0; k < 3; ++k) b.bm[k] = (uint32_t*)(m + lv_b + 2 * q_b + k * bm_b);
@@ -1043,16 +1108,18 @@ extern "C" int gbk_bfs_levels(gbk_matrix A, int64_t source, int direction, gbk_d
     rc = e == cudaSuccess ? GBK_SUCCESS : cuda_fail(e, "k_bfs1_init", __FILE__, __LINE__);
     count_launch(1);
     if (rc == GBK_SUCCESS)
-        rc = run_loop_graph(s, &st->cont, [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
+        rc = launch_loop(L, 0, s, &st->cont, [&](cudaStream_t cs, cudaGraphConditionalHandle h) {
             k_bfs1_light<<<grid, kT, 0, cs>>>(b, st);
             k_bfs1_heavy<<<grid, kT, 0, cs>>>(b, st);
             k_bfs1_control<<<1, 32, 0, cs>>>(st, b.n, h);
         });
-    if (rc == GBK_SUCCESS && !direct) {
+    if (rc == GBK_SUCCESS) {
+        // the levels into the caller's array in its type
 #define LV_OUT(TY) k_levels_out<TY><<<grid1(n), kT, 0, s>>>(b.lv, n, (TY*)levels)
         switch (level_type) {
             case GBK_F32: LV_OUT(float); break;
             case GBK_F64: LV_OUT(double); break;
+            case GBK_I32: LV_OUT(int32_t); break;
             default: LV_OUT(int64_t); break;
         }
 #undef LV_OUT
@@ -1067,7 +1134,6 @@ extern "C" int gbk_bfs_levels(gbk_matrix A, int64_t source, int direction, gbk_d
         if (e != cudaSuccess) rc = cuda_fail(e, "BFS depth", __FILE__, __LINE__);
         *depth = h.level;
     }
-    cudaFreeAsync(mem, s);
     return rc;
 }
 
@@ -1114,45 +1180,42 @@ extern "C" int gbk_pagerank(gbk_matrix A, int32_t itermax, double damping, doubl
         A->coldeg_zero = (int64_t)hz;
     }
     const int nb = blocks_for_sm((const void*)k_pr_post);
+    CachedLoop& L = single_cache(A).pr;
+    const size_t st_b = 256, v_b = 4 * (size_t)n, p_b = 4 * (size_t)nb;
+    int rc = loop_scratch(L, st_b + 4 * v_b + 2 * p_b);
+    if (rc) return rc;
     PrBufs b{};
     b.n = n;
     b.deg = A->coldeg;
-    b.damping = (float)damping;
-    b.inv_damping = (float)(1.0 / damping);
     b.nsinks = A->coldeg_zero;
     b.sparse_sink = A->coldeg_zero <= (int64_t)((double)n * 0.3) ? 1 : 0;
-    void* mem = nullptr;
-    const size_t st_b = 256, v_b = 4 * (size_t)n, p_b = 4 * (size_t)nb;
-    GBK_CUDA(cudaMallocAsync(&mem, st_b + 3 * v_b + 2 * p_b, s));
-    char* m = (char*)mem;
+    char* m = (char*)L.mem;
     PrState* st = (PrState*)m;
     m += st_b;
-    b.r[0] = ranks;
-    b.r[1] = (float*)m;
-    b.w = (float*)(m + v_b);
-    b.y = (float*)(m + 2 * v_b);
-    b.part_sink = (float*)(m + 3 * v_b);
-    b.part_diff = (float*)(m + 3 * v_b + p_b);
+    b.r[0] = (float*)m;
+    b.r[1] = (float*)(m + v_b);
+    b.w = (float*)(m + 2 * v_b);
+    b.y = (float*)(m + 3 * v_b);
+    b.part_sink = (float*)(m + 4 * v_b);
+    b.part_diff = (float*)(m + 4 * v_b + p_b);
     PrState h0{};
     h0.itermax = itermax;
     h0.tol = (float)tol;
     h0.scaled = (float)((1.0 - damping) / (double)n);
     h0.d_over_n = (float)(damping / (double)n);
     h0.rdiff = 1.0f;
-    int rc = GBK_SUCCESS;
+    h0.damping = (float)damping;
+    h0.inv_damping = (float)(1.0 / damping);
     auto fail = [&](cudaError_t e, const char* what) {
         if (rc == GBK_SUCCESS && e != cudaSuccess) rc = cuda_fail(e, what, __FILE__, __LINE__);
     };
     fail(cudaMemcpyAsync(st, &h0, sizeof(h0), cudaMemcpyHostToDevice, s), "gbk_pagerank state");
     if (rc == GBK_SUCCESS) {
-        k_pr_init<<<nb, kT, 0, s>>>(b, (float)(1.0 / (double)n));
+        k_pr_init<<<nb, kT, 0, s>>>(b, st, (float)(1.0 / (double)n));
         k_pr_control<<<1, 256, 0, s>>>(b, st, nb, 0, 0);
         fail(cudaGetLastError(), "k_pr_init");
         count_launch(2);
     }
-    // one iteration outside the graph: the first product also builds
-    // whatever the matrix's format builds on first use
-    PrState h{};
     auto iterate = [&](cudaStream_t cs, cudaGraphConditionalHandle hd) {
         int r = gbk_mxv(A, 0, GBK_PLUS_SECOND, GBK_OP_SECOND, GBK_F32, b.w, b.y, nullptr, GBK_F32, GBK_MASK_DEFAULT,
                         cs);
@@ -1161,34 +1224,35 @@ extern "C" int gbk_pagerank(gbk_matrix A, int32_t itermax, double damping, doubl
         count_launch(2);
         return r;
     };
-    if (rc == GBK_SUCCESS) {
+    PrState h{};
+    h.cont = itermax > 0 && !(tol > 0.0 && 1.0f < (float)tol) ? 1 : 0;
+    // The graph captures the SpMV of the matrix's current format; a new format
+    // (its generation) rebuilds it.  Before the first capture one iteration
+    // runs outside the graph: the first product also builds whatever the
+    // format builds on first use.
+    const bool cached = L.exec && L.key == A->format_gen && !host_loop_mode();
+    if (rc == GBK_SUCCESS && h.cont && !cached) {
+        rc = iterate(s, 0);
+        fail(cudaGetLastError(), "PageRank iteration");
         fail(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s), "gbk_pagerank state");
         fail(cudaStreamSynchronize(s), "gbk_pagerank state");
     }
     if (rc == GBK_SUCCESS && h.cont) {
-        rc = iterate(s, 0);
-        fail(cudaGetLastError(), "PageRank iteration");
-        if (rc == GBK_SUCCESS) {
-            fail(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s), "gbk_pagerank state");
-            fail(cudaStreamSynchronize(s), "gbk_pagerank state");
-        }
-    }
-    if (rc == GBK_SUCCESS && h.cont) {
         int irc = GBK_SUCCESS;
-        rc = run_loop_graph(s, &st->cont, [&](cudaStream_t cs, cudaGraphConditionalHandle hd) { irc = iterate(cs, hd); });
+        rc = launch_loop(L, A->format_gen, s, &st->cont,
+                         [&](cudaStream_t cs, cudaGraphConditionalHandle hd) { irc = iterate(cs, hd); });
         if (rc == GBK_SUCCESS) rc = irc;
-        if (rc == GBK_SUCCESS) {
-            fail(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s), "gbk_pagerank state");
-            fail(cudaStreamSynchronize(s), "gbk_pagerank state");
-        }
     }
-    if (rc == GBK_SUCCESS && h.cur == 1)
-        fail(cudaMemcpyAsync(ranks, b.r[1], v_b, cudaMemcpyDeviceToDevice, s), "gbk_pagerank ranks");
+    if (rc == GBK_SUCCESS) {
+        fail(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s), "gbk_pagerank state");
+        fail(cudaStreamSynchronize(s), "gbk_pagerank state");
+    }
+    if (rc == GBK_SUCCESS)
+        fail(cudaMemcpyAsync(ranks, b.r[h.cur & 1], v_b, cudaMemcpyDeviceToDevice, s), "gbk_pagerank ranks");
     if (rc == GBK_SUCCESS) {
         if (iters) *iters = h.iters;
         if (rdiff) *rdiff = h.rdiff;
     }
-    cudaFreeAsync(mem, s);
     return rc;
 }
 

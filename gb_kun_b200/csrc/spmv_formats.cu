@@ -1345,6 +1345,7 @@ int free_formats(gbk_matrix A) {
         A->lav[o] = nullptr;
     }
     A->format = GBK_FMT_CSR;
+    A->format_gen += 1;
     return GBK_SUCCESS;
 }
 
@@ -1398,6 +1399,7 @@ int build_format(gbk_matrix A, gbk_format fmt, const gbk_format_params* p, cudaS
         if (rc) return rc;
     }
     A->format = fmt;
+    A->format_gen += 1;
     return GBK_SUCCESS;
 }
 

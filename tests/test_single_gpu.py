@@ -442,3 +442,26 @@ def test_host_loop_mode_matches_graph_loop(torch, oracle, monkeypatch):
     assert a[5] == b[5] and np.array_equal(a[4], b[4])  # CSR SpMV: bit for bit
     A.close()
     Aw.close()
+
+
+def test_cached_loops_follow_format_changes(torch, oracle):
+    """The loops keep their scratch and graphs per matrix; PageRank's graph
+    holds the SpMV of the current format, so a new format must rebuild it."""
+    from conftest import REL_L1_TOL, rel_l1
+    g = gg.rmat(15, 16, seed=111)
+    A = _mat(g)
+    r = torch.zeros(g.n, device="cuda")
+    results = []
+    for fmt, kw in (("CSR", {}), ("SELL_C", {"seg_staged": 1, "reorder_cols": 1}), ("CSR_SEG", {}), ("CSR", {})):
+        A.set_format(fmt, **kw)
+        for _ in range(2):  # the second call runs the cached graph
+            it, _ = A.pagerank(r, itermax=50, damping=0.85, tol=1e-6)
+            r64, _, _ = oracle.pagerank(g, tol=0.0, itermax=it)
+            assert rel_l1(r.cpu().numpy(), r64) < REL_L1_TOL, fmt
+        results.append(it)
+    assert max(results) - min(results) <= 1
+    lv = torch.zeros(g.n, dtype=torch.int32, device="cuda")
+    for s in gg.sources(g, 3, seed=112):
+        A.bfs(int(s), lv)
+        assert np.array_equal(lv.cpu().numpy(), oracle.bfs(g, int(s)))
+    A.close()
