@@ -1284,24 +1284,22 @@ extern "C" int gbk_cc_labels(gbk_matrix A, gbk_dtype label_type, void* labels, v
     if (!direct) p = mode + 4;
     const unsigned g = grid1(n);
     k_cc_init<<<g, kT, 0, s>>>(p, n);
-    GBK_LAUNCHED();
     for (int r = 0; r < 2; ++r) {
         k_cc_link_entry<<<g, kT, 0, s>>>(A->csr.ptr, A->csr.idx, n, p, r);
-        GBK_LAUNCHED();
         k_cc_compress<<<g, kT, 0, s>>>(p, n);
-        GBK_LAUNCHED();
     }
     k_cc_sample_mode<<<1, 1024, 0, s>>>(p, n, mode);
-    GBK_LAUNCHED();
     k_cc_link_rest<<<blocks_for_sm((const void*)k_cc_link_rest), kT, 0, s>>>(A->csr.ptr, A->csr.idx, n, p, mode,
                                                                               sym ? 1 : 0);
-    GBK_LAUNCHED();
     switch (label_type) {
         case GBK_F32: k_cc_labels<float><<<g, kT, 0, s>>>(p, n, (float*)labels); break;
         case GBK_I32: k_cc_compress<<<g, kT, 0, s>>>(p, n); break;
         default: k_cc_labels<int64_t><<<g, kT, 0, s>>>(p, n, (int64_t*)labels); break;
     }
-    GBK_LAUNCHED();
+    count_launch(8);
+    // a failed launch leaves its error for this check; the scratch goes back either way
+    const cudaError_t e = cudaGetLastError();
     cudaFreeAsync(mode, s);
+    if (e != cudaSuccess) return cuda_fail(e, "gbk_cc_labels launch", __FILE__, __LINE__);
     return GBK_SUCCESS;
 }
