@@ -23,6 +23,7 @@ namespace gbk {
 namespace {
 
 constexpr int kBT = 256;  // threads per block of the persistent kernels
+constexpr int kBfsPiece = 256;  // entries per piece of a long row in the batched BFS push
 constexpr unsigned kFull = 0xffffffffu;
 
 int persistent_blocks(const void* kern, int threads) {
@@ -348,6 +349,8 @@ struct BfsCfg {
     unsigned long long* buf[2];
     int32_t* levels;
     int64_t stride;
+    int2* chunks;      // top-down: 256-entry pieces of rows longer than 32 entries, (vertex, first entry)
+    int32_t* nchunks;  // pieces appended this iteration
 };
 
 struct BfsState {
@@ -366,7 +369,9 @@ __device__ __forceinline__ int bfs_pick_pull(const BfsState* st, int cur_pull, i
 
 // Top-down step: each frontier vertex ORs its lane word into the next word
 // of every out-neighbour that some of those lanes have not visited.  Short
-// rows are walked by one thread, rows of more than 32 entries by the warp.
+// rows are walked by one thread; rows of more than 32 entries are cut into
+// 256-entry pieces that k_bfs_push_pieces hands out one per warp (a hub row
+// of 10^4 - 10^5 entries on one warp held the whole iteration back).
 __global__ void __launch_bounds__(kBT) k_bfs_push(const BfsCfg* __restrict__ cfg, const BfsState* __restrict__ st) {
     if (st->pull || st->st.active == 0) return;
     const int64_t n = cfg->n;
@@ -398,17 +403,46 @@ __global__ void __launch_bounds__(kBT) k_bfs_push(const BfsCfg* __restrict__ cfg
                 if (m) atomicOr(nx + u, m);
             }
         }
-        unsigned bigm = __ballot_sync(kFull, big);
-        while (bigm) {
-            const int src = __ffs(bigm) - 1;
-            bigm &= bigm - 1;
-            const unsigned long long ff = __shfl_sync(kFull, f, src);
-            const int32_t bb = __shfl_sync(kFull, b, src), ee = __shfl_sync(kFull, e, src);
-            for (int32_t k = bb + lane; k < ee; k += 32) {
-                const int32_t u = col[k];
-                const unsigned long long m = ff & ~vis[u];
-                if (m) atomicOr(nx + u, m);
-            }
+        // long rows: append their pieces, one atomic per warp
+        const int32_t np = big ? (e - b + kBfsPiece - 1) / kBfsPiece : 0;
+        int32_t incl = np;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int32_t total = __shfl_sync(kFull, incl, 31);
+        if (total) {
+            int32_t base0 = 0;
+            if (lane == 0) base0 = atomicAdd(cfg->nchunks, total);
+            base0 = __shfl_sync(kFull, base0, 0);
+            for (int32_t i = 0; i < np; ++i)
+                cfg->chunks[base0 + incl - np + i] = make_int2((int32_t)v, b + i * kBfsPiece);
+        }
+    }
+}
+
+// The pieces k_bfs_push appended, one warp per piece.
+__global__ void __launch_bounds__(kBT) k_bfs_push_pieces(const BfsCfg* __restrict__ cfg,
+                                                         const BfsState* __restrict__ st) {
+    if (st->pull || st->st.active == 0) return;
+    const int32_t np = *cfg->nchunks;
+    const int32_t* __restrict__ rp = cfg->rp;
+    const int32_t* __restrict__ col = cfg->col;
+    const int it = st->st.iter;
+    const unsigned long long* __restrict__ fr = cfg->buf[it & 1];
+    unsigned long long* nx = cfg->buf[(it + 1) & 1];
+    const unsigned long long* __restrict__ vis = cfg->visited;
+    const int lane = threadIdx.x & 31;
+    const int64_t wid = ((int64_t)blockIdx.x * kBT + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * kBT) >> 5;
+    for (int64_t c = wid; c < np; c += nwarps) {
+        const int2 pc = cfg->chunks[c];
+        const unsigned long long ff = fr[pc.x];
+        const int32_t ee = min(pc.y + kBfsPiece, rp[pc.x + 1]);
+        for (int32_t k = pc.y + lane; k < ee; k += 32) {
+            const int32_t u = col[k];
+            const unsigned long long m = ff & ~vis[u];
+            if (m) atomicOr(nx + u, m);
         }
     }
 }
@@ -529,7 +563,7 @@ __global__ void __launch_bounds__(kBT) k_bfs_finalize(const BfsCfg* __restrict__
     }
 }
 
-__global__ void k_bfs_control(BfsState* st, int64_t n, cudaGraphConditionalHandle h) {
+__global__ void k_bfs_control(BfsState* st, int64_t n, int32_t* nchunks, cudaGraphConditionalHandle h) {
     const int s = threadIdx.x;
     const unsigned long long act = st->st.active, alive = st->alive;
     if (s < 64 && ((act >> s) & 1) && ((alive >> s) & 1)) st->st.iters[s] += 1;
@@ -545,6 +579,7 @@ __global__ void k_bfs_control(BfsState* st, int64_t n, cudaGraphConditionalHandl
         st->last_n_front = st->n_front;
         st->pull = bfs_pick_pull(st, st->pull, n);
         st->alive = st->m_front = st->m_unvis = st->n_front = 0;
+        *nchunks = 0;
         const bool cont = st->st.active != 0 && st->st.launch_iters < st->launch_budget &&
                           !(st->stop_on_finish && fin);
         if (h) cudaGraphSetConditional(h, cont ? 1u : 0u);
@@ -597,12 +632,13 @@ struct BfsBatch final : Batch {
     BatchStatus* h_st = nullptr;
     int32_t* own_levels = nullptr;  // [64][n], allocated on the first admission into it
     LoopGraph loop;
-    int grid_push = 0, grid_pull = 0, grid_fin = 0;
+    int grid_push = 0, grid_pieces = 0, grid_pull = 0, grid_fin = 0;
     size_t bytes = 0;
 
     ~BfsBatch() override {
         cudaFree(cfg.visited);
         cudaFree(cfg.buf[0]);
+        cudaFree(cfg.nchunks);
         cudaFree(own_levels);
         cudaFree(d_cfg);
         cudaFree(d_st);
@@ -613,7 +649,7 @@ struct BfsBatch final : Batch {
     const BatchStatus* host() const override { return h_st; }
     size_t device_bytes() const override { return bytes; }
     size_t lane_bytes() const override { return (size_t)cfg.n * 4; }
-    int kernels_per_iter() const override { return 4; }
+    int kernels_per_iter() const override { return 5; }
 
     int init(gbk_matrix a, const BatchOptions& o, cudaStream_t s) {
         A = a;
@@ -634,6 +670,12 @@ struct BfsBatch final : Batch {
         cfg.stride = n;
         GBK_CUDA(cudaMemsetAsync(cfg.visited, 0, 8 * words, s));
         GBK_CUDA(cudaMemsetAsync(cfg.buf[0], 0, 16 * words, s));
+        // every vertex is in the frontier once per iteration, and a row of d > 32
+        // entries gives ceil(d / 256) <= d / 32 pieces: nnz / 32 + 1 bound them
+        const size_t npieces = (size_t)(A->csr.nnz / 32 + 1);
+        GBK_CUDA(cudaMalloc(&cfg.nchunks, 16 + sizeof(int2) * npieces));
+        GBK_CUDA(cudaMemsetAsync(cfg.nchunks, 0, 16, s));
+        cfg.chunks = reinterpret_cast<int2*>(reinterpret_cast<char*>(cfg.nchunks) + 16);
         GBK_CUDA(cudaMalloc(&d_cfg, sizeof(BfsCfg)));
         GBK_CUDA(cudaMalloc(&d_st, sizeof(BfsState)));
         GBK_CUDA(cudaMallocHost(&h_st, sizeof(BatchStatus)));
@@ -646,18 +688,21 @@ struct BfsBatch final : Batch {
         init.launch_budget = 1;
         GBK_CUDA(cudaMemcpyAsync(d_st, &init, sizeof(BfsState), cudaMemcpyHostToDevice, s));
         GBK_CUDA(cudaStreamSynchronize(s));
-        bytes = 8 * words * 3;
+        bytes = 8 * words * 3 + 16 + sizeof(int2) * npieces;
         grid_push = persistent_blocks((const void*)k_bfs_push, kBT);
+        grid_pieces = persistent_blocks((const void*)k_bfs_push_pieces, kBT);
         grid_pull = persistent_blocks((const void*)k_bfs_pull, kBT);
         grid_fin = persistent_blocks((const void*)k_bfs_finalize, kBT);
         return build_loop(loop, [this, n](cudaStream_t cs, cudaGraphConditionalHandle h) -> int {
             k_bfs_push<<<grid_push, kBT, 0, cs>>>(d_cfg, d_st);
             GBK_LAUNCH_CHECK();
+            k_bfs_push_pieces<<<grid_pieces, kBT, 0, cs>>>(d_cfg, d_st);
+            GBK_LAUNCH_CHECK();
             k_bfs_pull<<<grid_pull, kBT, 0, cs>>>(d_cfg, d_st);
             GBK_LAUNCH_CHECK();
             k_bfs_finalize<<<grid_fin, kBT, 0, cs>>>(d_cfg, d_st);
             GBK_LAUNCH_CHECK();
-            k_bfs_control<<<1, 64, 0, cs>>>(d_st, n, h);
+            k_bfs_control<<<1, 64, 0, cs>>>(d_st, n, cfg.nchunks, h);
             GBK_LAUNCH_CHECK();
             return GBK_SUCCESS;
         });
@@ -1181,7 +1226,7 @@ struct PprBatch final : Batch {
     const BatchStatus* host() const override { return h_st; }
     size_t device_bytes() const override { return bytes; }
     size_t lane_bytes() const override { return (size_t)cfg.n * 16; }
-    int kernels_per_iter() const override { return 4; }
+    int kernels_per_iter() const override { return 5; }
 
     int init(gbk_matrix a, const BatchOptions& o, cudaStream_t s) {
         A = a;
