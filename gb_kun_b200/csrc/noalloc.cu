@@ -26,7 +26,8 @@
 // kernels (cudaFuncGetAttributes), which loads them, so the array and the
 // code are resident before any caller runs out of memory.  The address is
 // cached per device.  A device that never saw gbk_init gets the same set-up
-// on its first call here; make that first call before any stream capture.
+// on its first call here (the calls synchronise their stream, so none of
+// them is ever inside a stream capture).
 // After cudaDeviceReset the module is loaded again and may move: call
 // gbk_init again, which refreshes the cached address.
 #include <atomic>

@@ -368,8 +368,9 @@ int gbk_vec_to_sparse(const void* dense, gbk_dtype t, int64_t n, int32_t* ids, v
  * loads this entry point's code and scratch on its device and caches the
  * scratch address, so the calls themselves allocate nothing; on a device
  * that never saw gbk_init the first call does that set-up (which may
- * allocate), so make it before any stream capture begins.  After
- * cudaDeviceReset call gbk_init again.  Synchronises the stream. */
+ * allocate).  After cudaDeviceReset call gbk_init again.  Synchronises the
+ * stream (it reads the count back), so it cannot be captured into a CUDA
+ * graph. */
 int gbk_vec_to_sparse_noalloc(const void* dense, gbk_dtype t, int64_t n, int32_t* ids, void* vals,
                               int64_t* nvals, void* stream);
 /* Sparse -> dense: zero fill, then scatter (DenseVector::convert, dense_vector.hpp:87-102). */
