@@ -33,6 +33,7 @@ CU_SOURCES = [
     "matrix.cu",
     "spmv_csr.cu",
     "spmv_bins.cu",
+    "spmv_chunks.cu",
     "spmv_formats.cu",
     "spmv_segsmem.cu",
     "spmv_sellw.cu",

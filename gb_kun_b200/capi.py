@@ -67,7 +67,7 @@ class TuneResult(C.Structure):
 
     CANDIDATES = ["CSR_bins", "CSR_merge", "SELL_C_s1", "SELL_C_s256", "SELL_C_s4096", "CSR_SEG", "LAV",
                   "SELL_C_s4096_hot16k", "SELL_C_s4096_hot52k", "SELL_C_s256_hot52k", "SELL_C_s4096_reorder",
-                  "SELL_C_s256_reorder", "SELL_C_staged", "SELL_C_staged_reorder"]
+                  "SELL_C_s256_reorder", "SELL_C_staged", "SELL_C_staged_reorder", "CSR_chunks"]
 
     def describe(self) -> dict:
         names = {0: "CSR", 3: "CSR_SEG", 4: "LAV", 6: "SELL_C"}
@@ -77,7 +77,7 @@ class TuneResult(C.Structure):
             d["hot_cols"] = self.sell_hot_cols
             d["staged_windows"] = bool(self.sell_staged)
         if self.format == 0:
-            d["csr_kernel"] = {1: "merge-path", 2: "degree-bins"}.get(self.csr_kernel, "default")
+            d["csr_kernel"] = {1: "merge-path", 2: "degree-bins", 3: "entry-chunks"}.get(self.csr_kernel, "default")
         if not self.cached:
             d["candidate_ms"] = {n: round(self.candidate_ms[i], 4) for i, n in enumerate(self.CANDIDATES)
                                  if i < self.ncandidates}
@@ -324,7 +324,8 @@ class Matrix:
 
     def set_format(self, fmt: str, sell_c=0, sigma=0, seg_cols=0, lav_frac=0.0, csr_kernel=0, hot_cols=0,
                    reorder_cols=0, seg_staged=0, stream=None):
-        """Storage format; csr_kernel picks the CSR kernel (0 default bins, 1 merge-path, 2 bins);
+        """Storage format; csr_kernel picks the CSR kernel (0 default bins, 1 merge-path, 2 bins,
+        3 runs of 256 entries per warp);
         hot_cols > 0 stages the x values of the most used columns in shared memory (SELL-C);
         reorder_cols renumbers columns by in-degree (SELL-C)."""
         p = FormatParams(sell_c, sigma, seg_cols, lav_frac, csr_kernel, hot_cols, reorder_cols, seg_staged)

@@ -15,15 +15,18 @@ constexpr int kSpmvThreads = 256;
 constexpr int kSpmvItems = 8;
 constexpr int kTileItems = kSpmvThreads * kSpmvItems;
 
-struct RowBins;  // spmv_bins.cu
+struct RowBins;    // spmv_bins.cu
+struct RowChunks;  // spmv_chunks.cu
 
-// CSR kernel choice of a view: degree-binned lane groups or merge-path tiles.
-enum { kKernelAuto = 0, kKernelMerge = 1, kKernelBins = 2 };
+// CSR kernel choice of a view: degree-binned lane groups, merge-path tiles or
+// equal runs of 256 entries per warp.
+enum { kKernelAuto = 0, kKernelMerge = 1, kKernelBins = 2, kKernelChunks = 3 };
 
 struct CsrView {
     int64_t nrows = 0, ncols = 0, nnz = 0;
     int kernel = kKernelAuto;
-    mutable RowBins* bins = nullptr;  // built on first use
+    mutable RowBins* bins = nullptr;      // built on first use
+    mutable RowChunks* chunks = nullptr;  // built on first use
     int32_t* ptr = nullptr;  // nrows + 1
     int32_t* idx = nullptr;  // nnz
     void* val = nullptr;     // nnz of the matrix value type
@@ -89,6 +92,11 @@ namespace gbk {
 
 int build_bins(const CsrView& v, int elem_bytes, RowBins** out, cudaStream_t s);
 void free_bins(RowBins* b);
+bool chunks_usable(const CsrView& v);
+int build_chunks(const CsrView& v, int elem_bytes, RowChunks** out, cudaStream_t s);
+void free_chunks(RowChunks* c);
+int spmv_chunks(const RowChunks* rc, const CsrView& v, int sr, int accum, int dtype, const void* x, void* y,
+                const void* mask, int mdt, int mmode, cudaStream_t s);
 int spmv_binned(const RowBins* rb, const CsrView& v, int sr, int accum, int dtype, const void* x, void* y,
                 const void* mask, int mdt, int mmode, cudaStream_t s);
 

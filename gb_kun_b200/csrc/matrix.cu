@@ -100,6 +100,7 @@ void free_view(CsrView& v) {
     cudaFree(v.carry_val);
     cudaFree(v.head_val);
     free_bins(v.bins);
+    free_chunks(v.chunks);
     v = CsrView{};
 }
 

@@ -9,7 +9,10 @@
 //                                                   one warp per chunk, partials folded
 //                                                   in chunk order by a small fix-up kernel
 // A block table maps every CTA of the single grid to its bin, so the whole
-// SpMV is two launches whatever the degree distribution.  Each group streams
+// SpMV is two launches whatever the degree distribution.  The heaviest bins
+// take the lowest CTA ids (split chunks, then warp rows, then the lane groups
+// from 32 down): CTAs start roughly in id order, so the longest work starts
+// first instead of in the grid's last wave.  Each group streams
 // its rows' col / val once (coalesced inside a row) and gathers x through L2.
 // This is the same computation as SpMV_all_active_diff_vectors
 // (src/backend/spmv/spmv_csr.h:340-384) with the reference's nnz-balanced
@@ -49,7 +52,8 @@ __host__ __device__ inline int bin_of_degree(int d) {
 }
 
 struct BinTable {
-    int32_t block_start[kNumBins + 1];  // CTA ranges per bin
+    int32_t block_start[kNumBins];      // CTA range [block_start, block_end) per bin
+    int32_t block_end[kNumBins];
     int32_t item_start[kNumBins];       // first item of the bin in perm (split bin: chunk table)
     int32_t items[kNumBins];            // rows (or chunks) in the bin
 };
@@ -148,7 +152,7 @@ __global__ void __launch_bounds__(kBinThreads) k_spmv_binned(
     int bin = 0;
 #pragma unroll
     for (int b = 1; b < kNumBins; b++)
-        if ((int)blockIdx.x >= bt.block_start[b]) bin = b;
+        if ((int)blockIdx.x >= bt.block_start[b] && (int)blockIdx.x < bt.block_end[b]) bin = b;
     const int lb = blockIdx.x - bt.block_start[bin];
     switch (bin) {
         case 0: {  // empty rows: the identity, accumulated
@@ -299,19 +303,20 @@ int build_bins(const CsrView& v, int elem_bytes, RowBins** out, cudaStream_t s) 
         GBK_CUDA(cudaMemcpyAsync(rb->split_first, split_first.data(), 4 * (rb->nsplit + 1), cudaMemcpyHostToDevice, s));
         GBK_CUDA(cudaStreamSynchronize(s));
     }
-    // block table
+    // block table: items in bin order (perm is sorted by bin), CTAs heaviest bin first
     int64_t blk = 0, item = 0;
     const int per_block[kNumBins] = {kBinThreads, kBinThreads, kBinThreads / 2, kBinThreads / 4, kBinThreads / 8,
                                      kBinThreads / 16, kBinThreads / 32, kBinThreads / 32, kBinThreads / 32};
     for (int b = 0; b < kNumBins; b++) {
-        const int64_t items = (b == kBinSplit) ? rb->nchunks : counts[b];
-        rb->bt.block_start[b] = (int32_t)blk;
         rb->bt.item_start[b] = (int32_t)item;
-        rb->bt.items[b] = (int32_t)items;
-        blk += (items + per_block[b] - 1) / per_block[b];
+        rb->bt.items[b] = (int32_t)((b == kBinSplit) ? rb->nchunks : counts[b]);
         item += counts[b];
     }
-    rb->bt.block_start[kNumBins] = (int32_t)blk;
+    for (int b = kNumBins - 1; b >= 0; b--) {
+        rb->bt.block_start[b] = (int32_t)blk;
+        blk += (rb->bt.items[b] + per_block[b] - 1) / per_block[b];
+        rb->bt.block_end[b] = (int32_t)blk;
+    }
     rb->blocks = blk;
     *out = rb;
     return GBK_SUCCESS;

@@ -260,6 +260,13 @@ int spmv_csr(const CsrView& v, int sr, int accum, int dtype, const void* x, void
              int mask_dtype, int mask_mode, cudaStream_t s) {
     GBK_REQUIRE(dtype == GBK_F32 || dtype == GBK_I32, GBK_UNSUPPORTED,
                 "spmv: element type %d unsupported (GBK_F32 or GBK_I32)", dtype);
+    if (v.kernel == kKernelChunks && assoc_semiring(sr) && v.nrows > 0 && chunks_usable(v)) {
+        if (!v.chunks) {
+            int rc = build_chunks(v, (int)dtype_size(dtype), &v.chunks, s);
+            if (rc) return rc;
+        }
+        return spmv_chunks(v.chunks, v, sr, accum, dtype, x, y, mask, mask_dtype, mask_mode, s);
+    }
     if (v.kernel != kKernelMerge && assoc_semiring(sr) && v.nrows > 0) {
         if (!v.bins) {
             int rc = build_bins(v, (int)dtype_size(dtype), &v.bins, s);

@@ -1363,7 +1363,7 @@ int build_format(gbk_matrix A, gbk_format fmt, const gbk_format_params* p, cudaS
                 prm.sell_c);
     GBK_REQUIRE(prm.sell_sigma >= 1 && prm.seg_cols >= 1 && prm.lav_dense_frac > 0.0f && prm.lav_dense_frac <= 1.0f,
                 GBK_INVALID_VALUE, "bad format parameters");
-    GBK_REQUIRE(prm.csr_kernel >= 0 && prm.csr_kernel <= kKernelBins, GBK_INVALID_VALUE, "bad csr_kernel %d",
+    GBK_REQUIRE(prm.csr_kernel >= 0 && prm.csr_kernel <= kKernelChunks, GBK_INVALID_VALUE, "bad csr_kernel %d",
                 prm.csr_kernel);
     GBK_REQUIRE(prm.seg_staged >= -1 && prm.seg_staged <= 1, GBK_INVALID_VALUE, "bad seg_staged %d",
                 prm.seg_staged);

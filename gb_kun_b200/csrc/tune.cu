@@ -36,6 +36,7 @@ const Candidate kCandidates[] = {
     {GBK_FMT_SELL_C, 4096, kKernelAuto, 53248}, {GBK_FMT_SELL_C, 256, kKernelAuto, 53248},
     {GBK_FMT_SELL_C, 4096, kKernelAuto, -1},    {GBK_FMT_SELL_C, 256, kKernelAuto, -1},
     {GBK_FMT_SELL_C, 0, kKernelAuto, 0, 1},     {GBK_FMT_SELL_C, 0, kKernelAuto, -1, 1},
+    {GBK_FMT_CSR, 0, kKernelChunks, 0},
 };
 constexpr int kNumCandidates = sizeof(kCandidates) / sizeof(kCandidates[0]);
 

@@ -33,7 +33,8 @@ typedef struct gbk_format_params {
     int32_t sell_sigma;      /* SELL-C sorting window in rows; default 4096; 1 = no sort */
     int32_t seg_cols;        /* CSR_SEG / LAV column-segment width; default 131072 (512 KiB of f32 x) */
     float lav_dense_frac;    /* LAV: fraction of nnz in the dense column segments; default 0.8 */
-    int32_t csr_kernel;      /* CSR kernel: 0 default (degree bins), 1 merge-path tiles, 2 degree bins */
+    int32_t csr_kernel;      /* CSR kernel: 0 default (degree bins), 1 merge-path tiles, 2 degree bins,
+                                3 equal runs of 256 entries per warp (column / value arrays 16-byte aligned) */
     int32_t sell_hot_cols;   /* SELL-C: columns renumbered by in-degree and the x values of the first
                                 sell_hot_cols (most used) columns staged in shared memory per CTA;
                                 0 = off; at most 53248 */
@@ -108,7 +109,8 @@ typedef struct gbk_tune_result {
     float candidate_ms[16];  /* CSR bins, CSR merge-path, SELL-C sigma 1 / 256 / 4096, CSR_SEG, LAV,
                                 SELL-C sigma 4096 with 16384 / 53248 hot columns, sigma 256 with 53248,
                                 SELL-C sigma 4096 / 256 with renumbered columns, SELL-C in staged x
-                                windows without / with renumbered columns; unused entries 0 */
+                                windows without / with renumbered columns, CSR in runs of 256 entries
+                                per warp; unused entries 0 */
     int32_t sell_hot_cols;   /* chosen hot-column count (SELL-C only; -1 = renumbered columns) */
     int32_t sell_staged;     /* 1 when the chosen SELL-C runs inside staged x windows */
 } gbk_tune_result;

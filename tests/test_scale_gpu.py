@@ -74,7 +74,7 @@ def rmat18():
     return g, gg.values_f32(g, seed=43), gg.vector_f32(g.n, seed=44)
 
 
-@pytest.mark.parametrize("kernel", [1, 2], ids=["merge", "bins"])
+@pytest.mark.parametrize("kernel", [1, 2, 3], ids=["merge", "bins", "chunks"])
 def test_csr_s18_vs_fp64_and_reference(torch, oracle, ref, rmat18, kernel):
     from gb_kun_b200 import capi
     g, val, x = rmat18
@@ -96,6 +96,7 @@ def test_csr_s18_vs_fp64_and_reference(torch, oracle, ref, rmat18, kernel):
 SWEEP = [
     ("CSR_bins", dict(fmt="CSR", csr_kernel=2)),
     ("CSR_merge", dict(fmt="CSR", csr_kernel=1)),
+    ("CSR_chunks", dict(fmt="CSR", csr_kernel=3)),
     ("SELL_C_s1", dict(fmt="SELL_C", sigma=1)),
     ("SELL_C_s256", dict(fmt="SELL_C", sigma=256)),
     ("SELL_C_s4096", dict(fmt="SELL_C", sigma=4096)),

@@ -38,7 +38,7 @@ def dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-KERNELS = [1, 2]  # merge-path tiles, degree bins
+KERNELS = [1, 2, 3]  # merge-path tiles, degree bins, runs of 256 entries per warp
 
 
 @pytest.mark.parametrize("kernel", KERNELS)
@@ -155,14 +155,83 @@ def test_errors_are_reported(capi):
     assert e.value.status == 7  # GBK_DOMAIN_MISMATCH (matrix f32, vectors i32)
 
 
-def test_repeatable(capi):
-    """Merge-path results do not depend on scheduling: two runs are identical."""
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_repeatable(capi, kernel):
+    """Results do not depend on scheduling: two runs are identical."""
     g = gg.rmat(14, 16, seed=61)
     val = gg.values_f32(g, seed=1)
     x = dev(gg.vector_f32(g.n, seed=2))
     A = capi.Matrix.from_graph(g, val)
+    A.set_format("CSR", csr_kernel=kernel)
     y1 = torch.empty(g.n, device="cuda")
     y2 = torch.empty(g.n, device="cuda")
     A.mxv(x, y1)
     A.mxv(x, y2)
     assert torch.equal(y1, y2)
+
+
+def _graph_from_lengths(lengths, seed):
+    """Rows of the given lengths, columns drawn without repeats per row."""
+    from gb_kun_b200.graphgen import Graph
+    lengths = np.asarray(lengths, np.int64)
+    n = max(len(lengths), int(lengths.max()) + 1 if len(lengths) else 1)
+    lengths = np.concatenate([lengths, np.zeros(n - len(lengths), np.int64)])
+    rng = np.random.default_rng(seed)
+    ptr = np.zeros(n + 1, np.int32)
+    ptr[1:] = np.cumsum(lengths)
+    col = np.concatenate([np.sort(rng.choice(n, size=int(k), replace=False)) for k in lengths if k > 0]
+                         or [np.zeros(0, np.int64)]).astype(np.int32)
+    return Graph(n=n, row_ptr=ptr, col=col)
+
+
+# Row lengths around the entry-chunk kernel's boundaries (256 entries per
+# warp, 8 per lane): rows ending exactly on a chunk / lane edge, rows spanning
+# many chunks (over 32: summed by a warp), chunks of more than 32 rows (row
+# search over several windows), empty rows between and at both ends, a last
+# chunk of 1..255.
+CHUNK_CASES = {
+    "aligned": [256, 256, 8, 248, 512],
+    "straddle": [0, 255, 2, 0, 0, 1, 300, 7, 9, 1, 0, 3000, 1, 1],
+    "empty_edges": [0, 0, 0, 17, 0, 1, 0, 2000, 0, 0],
+    "ragged_tail": [5] * 61 + [1],
+    "one_hub": [4099],
+    "two_hubs": [9000, 1, 8193, 8192, 8449],
+    "many_rows": [1] * 700 + [0] * 300 + [2] * 200,
+    "lane_edges": [8, 16, 7, 1, 9, 15, 24, 1, 255, 1, 257],
+}
+
+
+@pytest.mark.parametrize("case", sorted(CHUNK_CASES))
+@pytest.mark.parametrize("sr,dtype", [("plus_times", "f32"), ("min_plus", "i32"), ("lor_land", "f32")])
+def test_entry_chunks_row_boundaries(capi, oracle, case, sr, dtype):
+    g = _graph_from_lengths(CHUNK_CASES[case], seed=len(case))
+    if dtype == "f32":
+        val = gg.values_f32(g, seed=3) if g.nnz else np.zeros(0, np.float32)
+        x = gg.vector_f32(g.n, seed=4)
+    else:
+        val = gg.weights_i32(g, seed=3, lo=0, hi=50) if g.nnz else np.zeros(0, np.int32)
+        x = (gg.vector_f32(g.n, seed=4) * 100).astype(np.int32)
+    A = capi.Matrix.from_graph(g, val)
+    A.set_format("CSR", csr_kernel=3)
+    y0 = np.full(g.n, 2, val.dtype)
+    y = dev(y0)
+    A.mxv(dev(x), y, semiring=sr, accum="plus")
+    from gb_kun_b200.capi import BINOP
+    if sr == "plus_times":
+        expect = y0.astype(np.float64) + oracle.spmv_f64(g, val, x)
+        assert rel_l1(y.cpu().numpy(), expect) < REL_L1_TOL
+    else:
+        expect = oracle.mxv(sr, g, val, x, y0, accum=BINOP["plus"])
+        assert np.array_equal(y.cpu().numpy(), expect)
+    # the same rows under a mask, no accumulator
+    m = (np.arange(g.n) % 3) != 1
+    y = dev(y0)
+    A.mxv(dev(x), y, semiring=sr, mask=dev(m))
+    expect = oracle.mxv(sr, g, val, x, y0, mask=m)
+    if sr == "plus_times":
+        got = y.cpu().numpy()
+        assert np.all(got[~m] == 0)
+        ref = oracle.spmv_f64(g, val, x)
+        assert rel_l1(got[m], ref[m]) < REL_L1_TOL
+    else:
+        assert np.array_equal(y.cpu().numpy(), expect)
