@@ -66,6 +66,8 @@ def parse():
     p.add_argument("--staged", type=int, default=0,
                    help="--format SELL_C: 1 = SELL-C-sigma inside staged x windows; CSR_SEG / LAV: -1 = unstaged")
     p.add_argument("--reorder", type=int, default=0, help="--format SELL_C: renumber columns by in-degree")
+    p.add_argument("--csr-kernel", type=int, default=0,
+                   help="--format CSR: 0 default (degree bins), 1 merge-path, 2 degree bins, 3 runs of 256 entries")
     p.add_argument("--seed", type=int, default=42)
     p.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -265,9 +267,12 @@ def read_traffic(profile):
     return found.get("traffic_bytes_per_spmv:", found.get("traffic_bytes_per_launch:"))
 
 
-def dominant_kernel(fmt_name, scale, graph, staged=False):
+def dominant_kernel(fmt_name, scale, graph, staged=False, csr_kernel=0):
     """(kernel description, profile summary) for the storage format that ran."""
     tag = f"{graph}{scale}"
+    if fmt_name == "CSR" and csr_kernel == 3:
+        return ("k_spmv_chunks (256 entries per warp; + k_spmv_chunks_fixup for rows across chunks); achieved "
+                "counts the whole SpMV", f"spmv_csr_chunks_{tag}")
     if fmt_name == "SELL_C" and staged:
         return ("k_sellw (SELL-C-sigma inside x windows staged in shared memory; + k_sw_prologue for y and the "
                 "renumbered x); achieved counts the whole SpMV", f"spmv_sell_c_staged_{tag}")
@@ -309,6 +314,7 @@ def format_sweep(args, peak):
     O = Oracle()
     out = {}
     fmts = [("CSR_bins", {"fmt": "CSR", "csr_kernel": 2}), ("CSR_merge", {"fmt": "CSR", "csr_kernel": 1}),
+            ("CSR_chunks", {"fmt": "CSR", "csr_kernel": 3}),
             ("SELL_C_s1", {"fmt": "SELL_C", "sigma": 1}), ("SELL_C_s256", {"fmt": "SELL_C", "sigma": 256}),
             ("SELL_C_s4096", {"fmt": "SELL_C", "sigma": 4096}),
             ("SELL_C_s4096_reorder", {"fmt": "SELL_C", "sigma": 4096, "reorder": 1}),
@@ -491,7 +497,8 @@ def run_ours(args):
         if args.format == "auto":
             tuned = A.autotune(reps=20).describe()
         else:
-            A.set_format(args.format, sigma=args.sigma, seg_staged=args.staged, reorder_cols=args.reorder)
+            A.set_format(args.format, sigma=args.sigma, seg_staged=args.staged, reorder_cols=args.reorder,
+                         csr_kernel=args.csr_kernel)
         for _ in range(args.warmup):
             A.mxv(dx, dy)
         torch.cuda.synchronize()
@@ -530,7 +537,10 @@ def run_ours(args):
     peak, peak_kind = hbm_peak()
     ran_format = tuned["format"] if tuned else args.format
     staged = bool(tuned.get("staged_windows")) if tuned else args.staged == 1
-    kern_desc, kern_profile = dominant_kernel(ran_format, args.scale, args.graph, staged)
+    ran_csr_kernel = tuned.get("csr_kernel") if tuned else args.csr_kernel
+    ran_csr_kernel = {"entry-chunks": 3}.get(ran_csr_kernel, ran_csr_kernel)
+    kern_desc, kern_profile = dominant_kernel(ran_format, args.scale, args.graph, staged,
+                                              ran_csr_kernel if isinstance(ran_csr_kernel, int) else 0)
     # one launch = one SpMV (the y initialisation and the main kernel, which
     # starts under programmatic dependent launch); its average duration is
     # the per-step time of the timed region
