@@ -314,20 +314,27 @@ bool chunks_usable(const CsrView& v) {
     return ((uintptr_t)v.idx % 16) == 0 && ((uintptr_t)v.val % 16) == 0;
 }
 
-int build_chunks(const CsrView& v, int elem_bytes, RowChunks** out, cudaStream_t s) {
-    GBK_REQUIRE(chunks_usable(v), GBK_INVALID_VALUE, "entry-chunk SpMV: column / value arrays not 16-byte aligned");
-    GBK_REQUIRE(v.nrows > 0, GBK_INVALID_VALUE, "entry-chunk SpMV: no rows");
+namespace {
+
+// Stream-ordered temporaries released on every return path.
+struct Scratch {
+    cudaStream_t s;
+    void* p[4] = {nullptr, nullptr, nullptr, nullptr};
+    explicit Scratch(cudaStream_t st) : s(st) {}
+    ~Scratch() {
+        for (void* q : p)
+            if (q) cudaFreeAsync(q, s);
+    }
+};
+
+int fill_chunks(const CsrView& v, int elem_bytes, RowChunks* rc, cudaStream_t s) {
     const int64_t n = v.nrows, nnz = v.nnz;
-    RowChunks* rc = new RowChunks();
     rc->nchunks = (nnz + kChunk - 1) / kChunk;
-    int32_t *flag = nullptr, *pos = nullptr, *counts = nullptr;
-    void* tmp = nullptr;
+    Scratch sc(s);
     size_t tb = 0;
-    GBK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag, pos, (int)n, s));
-    GBK_CUDA(cudaMallocAsync(&flag, 4 * n, s));
-    GBK_CUDA(cudaMallocAsync(&pos, 4 * n, s));
-    GBK_CUDA(cudaMallocAsync(&counts, 12, s));
-    GBK_CUDA(cudaMallocAsync(&tmp, tb, s));
+    GBK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, (const int32_t*)nullptr, (int32_t*)nullptr, (int)n, s));
+    for (int i = 0; i < 4; i++) GBK_CUDA(cudaMallocAsync(&sc.p[i], i == 2 ? 12 : i == 3 ? tb : 4 * (size_t)n, s));
+    int32_t *flag = (int32_t*)sc.p[0], *pos = (int32_t*)sc.p[1], *counts = (int32_t*)sc.p[2];
     GBK_CUDA(cudaMemsetAsync(counts, 0, 12, s));
     GBK_CUDA(cudaMalloc(&rc->rows, 4 * n));
     GBK_CUDA(cudaMalloc(&rc->rptr, 4 * (n + 1)));
@@ -336,7 +343,7 @@ int build_chunks(const CsrView& v, int elem_bytes, RowChunks** out, cudaStream_t
     const unsigned g = (unsigned)((n + 255) / 256);
     k_row_flags<<<g, 256, 0, s>>>(v.ptr, n, flag);
     GBK_LAUNCHED();
-    GBK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, flag, pos, (int)n, s));
+    GBK_CUDA(cub::DeviceScan::ExclusiveSum(sc.p[3], tb, flag, pos, (int)n, s));
     count_launch(1);
     k_row_split<<<g, 256, 0, s>>>(v.ptr, n, flag, pos, rc->rows, rc->rptr, rc->empty_rows, counts);
     GBK_LAUNCHED();
@@ -359,10 +366,20 @@ int build_chunks(const CsrView& v, int elem_bytes, RowChunks** out, cudaStream_t
         GBK_CUDA(cudaStreamSynchronize(s));
         rc->nlong = h[2];
     }
-    cudaFreeAsync(flag, s);
-    cudaFreeAsync(pos, s);
-    cudaFreeAsync(counts, s);
-    cudaFreeAsync(tmp, s);
+    return GBK_SUCCESS;
+}
+
+}  // namespace
+
+int build_chunks(const CsrView& v, int elem_bytes, RowChunks** out, cudaStream_t s) {
+    GBK_REQUIRE(chunks_usable(v), GBK_INVALID_VALUE, "entry-chunk SpMV: column / value arrays not 16-byte aligned");
+    GBK_REQUIRE(v.nrows > 0, GBK_INVALID_VALUE, "entry-chunk SpMV: no rows");
+    RowChunks* rc = new RowChunks();
+    const int st = fill_chunks(v, elem_bytes, rc, s);
+    if (st != GBK_SUCCESS) {
+        free_chunks(rc);
+        return st;
+    }
     *out = rc;
     return GBK_SUCCESS;
 }
