@@ -34,7 +34,10 @@ typedef struct gbk_format_params {
     int32_t seg_cols;        /* CSR_SEG / LAV column-segment width; default 131072 (512 KiB of f32 x) */
     float lav_dense_frac;    /* LAV: fraction of nnz in the dense column segments; default 0.8 */
     int32_t csr_kernel;      /* CSR kernel: 0 default (degree bins), 1 merge-path tiles, 2 degree bins,
-                                3 equal runs of 256 entries per warp (column / value arrays 16-byte aligned) */
+                                3 equal runs of 256 entries per warp (needs 16-byte aligned column / value
+                                arrays, which the library's own allocations always are; otherwise, and
+                                for semirings whose add is not associative, the degree bins or the
+                                in-order row kernel run) */
     int32_t sell_hot_cols;   /* SELL-C: columns renumbered by in-degree and the x values of the first
                                 sell_hot_cols (most used) columns staged in shared memory per CTA;
                                 0 = off; at most 53248 */
