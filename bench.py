@@ -267,10 +267,11 @@ def read_traffic(profile):
     return found.get("traffic_bytes_per_spmv:", found.get("traffic_bytes_per_launch:"))
 
 
-def dominant_kernel(fmt_name, scale, graph, staged=False, csr_kernel=0):
-    """(kernel description, profile summary) for the storage format that ran."""
+def dominant_kernel(fmt_name, scale, graph, staged=False, csr_kernel=0, nnz=0):
+    """(kernel description, profile summary) for the storage format that ran
+    (the default CSR kernel takes runs of 256 entries from 2^23 entries on)."""
     tag = f"{graph}{scale}"
-    if fmt_name == "CSR" and csr_kernel == 3:
+    if fmt_name == "CSR" and (csr_kernel == 3 or (csr_kernel == 0 and nnz >= 1 << 23)):
         return ("k_spmv_chunks (256 entries per warp; + k_spmv_chunks_fixup for rows across chunks); achieved "
                 "counts the whole SpMV", f"spmv_csr_chunks_{tag}")
     if fmt_name == "SELL_C" and staged:
@@ -550,7 +551,7 @@ def run_ours(args):
     ran_csr_kernel = tuned.get("csr_kernel") if tuned else args.csr_kernel
     ran_csr_kernel = {"entry-chunks": 3}.get(ran_csr_kernel, ran_csr_kernel)
     kern_desc, kern_profile = dominant_kernel(ran_format, args.scale, args.graph, staged,
-                                              ran_csr_kernel if isinstance(ran_csr_kernel, int) else 0)
+                                              ran_csr_kernel if isinstance(ran_csr_kernel, int) else 0, g.nnz)
     # one launch = one SpMV (the y initialisation and the main kernel, which
     # starts under programmatic dependent launch); its average duration is
     # the per-step time of the timed region

@@ -324,8 +324,8 @@ class Matrix:
 
     def set_format(self, fmt: str, sell_c=0, sigma=0, seg_cols=0, lav_frac=0.0, csr_kernel=0, hot_cols=0,
                    reorder_cols=0, seg_staged=0, stream=None):
-        """Storage format; csr_kernel picks the CSR kernel (0 default bins, 1 merge-path, 2 bins,
-        3 runs of 256 entries per warp);
+        """Storage format; csr_kernel picks the CSR kernel (0 default: bins, or runs of 256 entries
+        for unmasked products over 2^23+ entries; 1 merge-path, 2 bins, 3 runs of 256 entries per warp);
         hot_cols > 0 stages the x values of the most used columns in shared memory (SELL-C);
         reorder_cols renumbers columns by in-degree (SELL-C)."""
         p = FormatParams(sell_c, sigma, seg_cols, lav_frac, csr_kernel, hot_cols, reorder_cols, seg_staged)

@@ -254,13 +254,20 @@ int dispatch(const CsrView& v, int sr, int accum, const void* x, void* y, const 
 
 }  // namespace
 
+constexpr int64_t kChunksAutoNnz = 1ll << 23;
+
 static bool assoc_semiring(int sr) { return sr != GBK_FIRST_WINS && sr != GBK_CUSTOM_LESS_PLUS; }
 
 int spmv_csr(const CsrView& v, int sr, int accum, int dtype, const void* x, void* y, const void* mask,
              int mask_dtype, int mask_mode, cudaStream_t s) {
     GBK_REQUIRE(dtype == GBK_F32 || dtype == GBK_I32, GBK_UNSUPPORTED,
                 "spmv: element type %d unsupported (GBK_F32 or GBK_I32)", dtype);
-    if (v.kernel == kKernelChunks && assoc_semiring(sr) && v.nrows > 0 && chunks_usable(v)) {
+    // the default kernel: degree bins, except unmasked products over large
+    // matrices, where equal runs of entries measured faster (R-MAT: 0.248
+    // against 0.28 ms at 65 M entries, 65 against 72 us at 16 M, slower at
+    // 4 M); a mask keeps the bins, which skip masked-out rows before any load
+    const bool auto_chunks = v.kernel == kKernelAuto && !mask && v.nnz >= kChunksAutoNnz;
+    if ((v.kernel == kKernelChunks || auto_chunks) && assoc_semiring(sr) && v.nrows > 0 && chunks_usable(v)) {
         if (!v.chunks) {
             int rc = build_chunks(v, (int)dtype_size(dtype), &v.chunks, s);
             if (rc) return rc;

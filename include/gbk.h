@@ -33,7 +33,8 @@ typedef struct gbk_format_params {
     int32_t sell_sigma;      /* SELL-C sorting window in rows; default 4096; 1 = no sort */
     int32_t seg_cols;        /* CSR_SEG / LAV column-segment width; default 131072 (512 KiB of f32 x) */
     float lav_dense_frac;    /* LAV: fraction of nnz in the dense column segments; default 0.8 */
-    int32_t csr_kernel;      /* CSR kernel: 0 default (degree bins), 1 merge-path tiles, 2 degree bins,
+    int32_t csr_kernel;      /* CSR kernel: 0 default (degree bins; unmasked products over matrices of
+                                2^23 or more entries use kernel 3), 1 merge-path tiles, 2 degree bins,
                                 3 equal runs of 256 entries per warp (needs 16-byte aligned column / value
                                 arrays, which the library's own allocations always are; otherwise, and
                                 for semirings whose add is not associative, the degree bins or the

@@ -50,3 +50,13 @@ def test_default_line_profile_matches_the_tree():
     assert "k_sellw" in kern
     t = bench.read_traffic(prof)
     assert t is not None and 4e8 < t < 6e8, (prof, t)
+
+
+def test_csr_line_names_the_kernel_that_runs():
+    # the default CSR kernel takes runs of 256 entries from 2^23 entries on
+    kern, prof = bench.dominant_kernel("CSR", 22, "rmat", csr_kernel=0, nnz=65_243_159)
+    assert "k_spmv_chunks" in kern and prof == "spmv_csr_chunks_rmat22"
+    kern, prof = bench.dominant_kernel("CSR", 18, "rmat", csr_kernel=0, nnz=3_937_938)
+    assert "k_spmv_binned" in kern
+    kern, _ = bench.dominant_kernel("CSR", 22, "rmat", csr_kernel=2, nnz=65_243_159)
+    assert "k_spmv_binned" in kern
